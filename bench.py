@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Radix-join benchmark on B200.
+
+Default workload (the large in-HBM radix join): R = 2^30 tuples (int64 key,
+int64 payload) with keys a seeded permutation of 1..2^30, S = 2^30 tuples with
+foreign keys drawn from R's keys (Zipf exponent --zipf, 0 = uniform),
+payload = key, two radix passes of 9 + 9 bits, bucket-chaining shared-memory
+join.  One step = one whole join (prefix sums, both partition passes, join,
+result reduction) through the library's engine.  value = (|R| + |S|) / step
+time in G tuples/s, inputs resident in HBM (34 GB, larger than L2, so no L2
+flush is needed between steps).  e2e = the same join through the C ABI's
+host-buffer entry point, with the four input columns copied from pinned host
+memory and the result copied back inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU radix join (its own compiled CPU
+partitioner for pass 1, the oracle restatement for pass 2 and the join) on all
+host cores over a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "fast-interconnects_b200"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+METRIC = "radix join G tuples/s"
+UNIT = "G tuples/s"
+# Algorithmic bytes per tuple of a P-pass radix join: key read for the
+# histogram, P scatter round trips, one join read: K + P*2T + T.
+KEY_B, TUPLE_B = 8, 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log2n", type=int, default=30, help="|R| = |S| = 2^log2n")
+    ap.add_argument("--zipf", type=float, default=0.0)
+    ap.add_argument("--bits", default="9,9")
+    ap.add_argument("--scheme", default="chaining", choices=["chaining", "perfect"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-log2n", type=int, default=27,
+                    help="CPU baseline sample: |R| = |S| = 2^cpu_log2n")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=2026)
+    return ap.parse_args()
+
+
+def workload_name(a):
+    n = 1 << a.log2n
+    bits = "+".join(a.bits.split(","))
+    skew = "uniform" if a.zipf == 0 else "zipf%.1f" % a.zipf
+    return "radix_join_%dMx%dM_int64_%sbits_%s_%s" % (n >> 20, n >> 20, bits,
+                                                     skew, a.scheme)
+
+
+def load_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM traffic per launch of the dominant kernels from the committed ncu
+    summary (profiles/traffic.json), if present."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        if torch.cuda.is_available():
+            torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gen_relations(fi, torch, n, zipf, seed):
+    rk = torch.empty(n, dtype=torch.int64, device="cuda")
+    sk = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_primary_keys(rk, seed, base=1)
+    fi.gen_zipf_foreign_keys(sk, n, zipf, seed + 1, seed, base=1)
+    return rk, sk
+
+
+def cpu_baseline(a, fi, torch):
+    """The reference CPU radix join on a bounded sample, all host cores."""
+    import numpy as np
+    import oracle as O
+    n = 1 << a.cpu_log2n
+    b1, b2 = [int(x) for x in a.bits.split(",")]
+    if torch.cuda.is_available():
+        rk, sk = gen_relations(fi, torch, n, a.zipf, a.seed)
+        r = rk.cpu().numpy()
+        s = sk.cpu().numpy()
+        del rk, sk
+    else:
+        r = O.primary_keys(n, a.seed, np.int64)
+        s = O.zipf_foreign_keys(n, n, a.zipf, a.seed + 1, a.seed, np.int64)
+    threads = os.cpu_count() or 1
+    times = []
+    res = None
+    for _ in range(2):
+        t0 = time.perf_counter()
+        res = O.cpu_radix_join(r, r, s, s, b1, b2, threads, use_reference=True)
+        times.append(time.perf_counter() - t0)
+    sm, cnt, phases, kind = res
+    assert cnt == n, "CPU baseline lost matches"
+    best = min(times)
+    return {"value": 2 * n / best / 1e9, "unit": UNIT, "cores": threads,
+            "kind": kind,
+            "sample": "R=S=2^%d int64 tuples (same generator and seeds), %s+%s bits, "
+                      "pass 1 = reference cpu_chunked_prefix_sum + "
+                      "cpu_chunked_radix_partition_swwc (one chunk per thread), "
+                      "pass 2 + bucket-chaining join = oracle restatement; best of 2"
+                      % (a.cpu_log2n, b1, b2),
+            "seconds": best}
+
+
+def run_reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle as O
+    try:
+        import torch
+        import fi_sqlops as fi
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        have_gpu = False
+    n = 1 << a.cpu_log2n
+    b1, b2 = [int(x) for x in a.bits.split(",")]
+    if have_gpu:
+        torch.cuda.set_device(0)
+        rk, sk = gen_relations(fi, torch, n, a.zipf, a.seed)
+        r, s = rk.cpu().numpy(), sk.cpu().numpy()
+        del rk, sk
+        torch.cuda.empty_cache()
+    else:
+        r = O.primary_keys(n, a.seed, np.int64)
+        s = O.zipf_foreign_keys(n, n, a.zipf, a.seed + 1, a.seed, np.int64)
+    threads = os.cpu_count() or 1
+    kind = None
+    for _ in range(a.warmup):
+        O.cpu_radix_join(r, r, s, s, b1, b2, threads, use_reference=True)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        sm, cnt, _, kind = O.cpu_radix_join(r, r, s, s, b1, b2, threads,
+                                            use_reference=True)
+        times.append(time.perf_counter() - t0)
+    assert cnt == n
+    t = sum(times) / len(times)
+    value = 2 * n / t / 1e9
+    sample = ("R=S=2^%d int64 (bounded sample of %s), %s+%s bits, %d host threads; "
+              "pass 1 = reference CPU partitioner compiled from its sources, "
+              "pass 2 + join = oracle restatement" % (a.cpu_log2n, workload_name(a),
+                                                      b1, b2, threads))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded permutation PK, Zipf/uniform FK)",
+            "config": {"workload": workload_name(a), "sample_tuples": 2 * n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+PHASES = [  # (name, event pairs, algorithmic bytes per tuple of the relation)
+    ("pass1_histogram", [(0, 1), (4, 5)], KEY_B),
+    ("pass1_scatter", [(1, 2), (5, 6)], 2 * TUPLE_B),
+    ("pass2_histogram", [(2, 3), (6, 7)], TUPLE_B),
+    ("pass2_scatter", [(3, 4), (7, 8)], 2 * TUPLE_B),
+    ("join", [(8, 9)], TUPLE_B),
+]
+
+
+def run_ours(a):
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    n = 1 << a.log2n
+    bits = [int(x) for x in a.bits.split(",")]
+    passes = len(bits)
+    rb = fi.RadixBits(*bits)
+    scheme = fi.HashingScheme.BucketChaining if a.scheme == "chaining" else \
+        fi.HashingScheme.Perfect
+    seed = a.seed + 1000 * rank
+    rk, sk = gen_relations(fi, torch, n, a.zipf, seed)
+    expected_sum = int(sk.sum().item())
+    engine = fi.RadixJoinEngine(n, n, torch.int64, rb, scheme)
+    stream = torch.cuda.current_stream()
+
+    # warm-up (untimed), checked against the closed form: every S key is a
+    # foreign key, so count = |S| and sum = sum(S.payload)
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        s, c = engine.run(rk, rk, sk, sk)
+        verified = verified and (c == n and s == expected_sum)
+    engine.status()
+
+    K = a.steps
+    ev_sets = []
+    for _ in range(K):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(11)]
+        for e in evs:
+            e.record(stream)
+        ev_sets.append(evs)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        start.record(stream)
+        for k in range(K):
+            engine.set_events(ev_sets[k])
+            engine.run_async(rk, rk, sk, sk)
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    engine.set_events(None)
+    clocks = clk.summary()
+    elapsed_ms = start.elapsed_time(end)
+    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    launches = engine.last_launches() * K
+    r = engine.result.cpu()
+    verified = verified and int(r[1]) == n and int(r[0]) == expected_sum
+    ms_per_step = elapsed_ms / K
+    value = world * 2 * n * K / (elapsed_ms / 1e3) / 1e9
+
+    # per-phase device times from the events recorded on the launching stream
+    peak, peak_kind = load_peaks()
+    phases = {}
+    for name, pairs, bpt in PHASES:
+        if passes == 1 and name.startswith("pass2"):
+            continue
+        t = statistics.mean(sum(ev[b].elapsed_time(ev[e]) for b, e in pairs)
+                            for ev in ev_sets)
+        nbytes = 2 * n * bpt
+        phases[name] = {"ms": t, "gb_per_s": nbytes / (t / 1e3) / 1e9,
+                        "algorithmic_bytes": nbytes}
+    dominant = max(phases, key=lambda k: phases[k]["ms"])
+    d = phases[dominant]
+    traffic = load_traffic().get(dominant)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": d["gb_per_s"],
+                "peak": peak, "unit": "GB/s", "frac": d["gb_per_s"] / peak,
+                "peak_source": peak_kind,
+                "traffic": traffic,
+                "launch_ms": d["ms"] / 2 if dominant != "join" else d["ms"],
+                "algorithmic_bytes_per_launch":
+                    d["algorithmic_bytes"] // (1 if dominant == "join" else 2)}
+    pipe_bytes = 2 * n * (KEY_B + passes * 2 * TUPLE_B + TUPLE_B)
+    pipeline = {"algorithmic_bytes_per_step": pipe_bytes,
+                "achieved_gb_per_s": pipe_bytes / (ms_per_step / 1e3) / 1e9,
+                "frac_of_peak": pipe_bytes / (ms_per_step / 1e3) / 1e9 / peak}
+
+    # e2e through the host-buffer entry point
+    e2e = None
+    if not a.no_e2e and a.e2e_steps > 0:
+        hk = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        hs = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        hk.copy_(rk)
+        hs.copy_(sk)
+        del rk, sk
+        torch.cuda.empty_cache()
+        engine.run_host(hk, hk, hs, hs)  # warm-up (allocates device columns)
+        t_e2e = []
+        for _ in range(a.e2e_steps):
+            barrier(world)
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            s, c = engine.run_host(hk, hk, hs, hs)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            verified = verified and c == n and s == expected_sum
+            t_e2e.append(t0.elapsed_time(t1))
+        e2e_ms = max_over_ranks(statistics.mean(t_e2e), world)
+        e2e = {"value": world * 2 * n / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 16,
+               "ms_per_step": e2e_ms,
+               "path": "fi_radix_join_engine_run_host_int64 (pinned host columns)"}
+        del hk, hs
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a, fi, torch)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": K, "warmup": a.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int64",
+                "data": "synthetic (seeded permutation PK 1..N, Zipf(s)/uniform FK, "
+                        "payload = key)",
+                "config": {"workload": workload_name(a), "build_tuples": n,
+                           "probe_tuples": n, "radix_bits": bits,
+                           "hashing_scheme": a.scheme, "zipf_s": a.zipf,
+                           "l2_flush": "none: inputs (%d GB) larger than L2"
+                                       % (4 * n * 8 // 10**9),
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "roofline": roofline, "pipeline_roofline": pipeline,
+                "phases": phases, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clocks,
+                "verified": bool(verified),
+                "workspace_gb": engine.workspace_bytes() / 1e9}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

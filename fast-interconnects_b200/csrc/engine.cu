@@ -1,0 +1,555 @@
+// The radix-join execution method on one B200
+// (radix-join/src/execution_methods/gpu_radix_join.rs:90-565).
+//
+// The reference runs pass 1 for R and S and then loops over the 2^b1
+// first-pass partitions on two streams, issuing six launches per partition
+// (two prefix_sum_and_transform gathers, two second-pass partitions, task
+// assignment, join), i.e. about 3000 launches at 9+9 bits, each with a grid of
+// half the GPU.  This engine instead runs every step over all partitions at
+// once, so the whole join is about a dozen launches that each fill the GPU:
+//
+//   1. Chunked histograms + offsets of R and S on the first-pass bits.
+//   2. Tile scatter of R and S into chunked AoS relations (pass 1).
+//   3. Plan: per first-pass partition p1, its length (summed over chunks),
+//      its start in the pass-2 output and its split into "pieces" of at most
+//      kPieceTuples tuples.  Pieces are the unit of pass-2 work, so a
+//      Zipf-hot partition is spread over many CTAs.
+//   4. Piece histograms on the second-pass bits (reads the pass-1 output).
+//   5. Cursors: per (p1, p2) the contiguous output offsets, per piece its
+//      cursor inside each (p1, p2) sub-partition.
+//   6. Tile scatter of every piece into the final layout, ordered by
+//      (p1, p2) with no padding (this replaces the reference's AoS->SoA
+//      transform copy plus the second-pass prefix sum and partition).
+//   7. One shared-memory join over all 2^(b1+b2) partitions (join.cu), then
+//      a reduction of the per-thread sums into {sum, count}.
+// With a single pass (b2 absent) steps 3-6 are skipped and pass 1 uses the
+// Contiguous layout, as the join requires.
+#include <algorithm>
+#include <cstring>
+
+#include "../../include/fi_sqlops.h"
+#include "api_internal.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "tile_scatter.cuh"
+
+namespace fi {
+
+constexpr uint64_t kPieceTuples = 1ull << 19;
+constexpr uint32_t kJoinBlock = 1024;
+
+struct Pass2Plan {
+  uint64_t *reg_pre;      // [F1][C1+1] prefix of the chunk regions of p1
+  uint64_t *p1_base;      // [F1+1] start of p1 in the pass-2 output
+  uint32_t *piece_first;  // [F1+1] first piece of p1
+  uint32_t *hist;         // [max_pieces][F2]
+  uint64_t *cursor;       // [max_pieces][F2]
+  uint64_t *off2;         // [F1*F2 + 1]
+};
+
+// Exclusive scan of a global u64 array by one CTA; a[n] gets the total.
+__device__ void cta_scan_global_u64(uint64_t *a, uint32_t n, uint64_t *tmp) {
+  uint64_t carry = 0;
+  for (uint32_t base = 0; base < n; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint64_t v = i < n ? a[i] : 0;
+    uint64_t total;
+    const uint64_t ex = block_exclusive_scan_u64(v, tmp, &total);
+    if (i < n) a[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) a[n] = carry;
+}
+
+__global__ void __launch_bounds__(1024)
+    pass2_plan_kernel(const uint64_t *__restrict__ off1, uint32_t C1,
+                      uint32_t F1, uint64_t padded1, uint32_t pad,
+                      Pass2Plan pl, uint64_t *piece_count_tmp) {
+  __shared__ uint64_t tmp[33];
+  const uint64_t n_off = (uint64_t)C1 * F1;
+  for (uint32_t p1 = threadIdx.x; p1 < F1; p1 += blockDim.x) {
+    uint64_t run = 0;
+    uint64_t *rp = pl.reg_pre + (uint64_t)p1 * (C1 + 1);
+    for (uint32_t c = 0; c < C1; ++c) {
+      const uint64_t ofi = (uint64_t)c * F1 + p1;
+      const uint64_t b = off1[ofi];
+      const uint64_t e = (ofi + 1 < n_off) ? off1[ofi + 1] - pad : padded1;
+      rp[c] = run;
+      run += e - b;
+    }
+    rp[C1] = run;
+    pl.p1_base[p1] = run;
+    piece_count_tmp[p1] = (run + kPieceTuples - 1) / kPieceTuples;
+  }
+  __syncthreads();
+  cta_scan_global_u64(pl.p1_base, F1, tmp);
+  __syncthreads();
+  cta_scan_global_u64(piece_count_tmp, F1, tmp);
+  __syncthreads();
+  for (uint32_t p1 = threadIdx.x; p1 <= F1; p1 += blockDim.x)
+    pl.piece_first[p1] = (uint32_t)piece_count_tmp[p1];
+}
+
+__device__ __forceinline__ uint32_t find_p1(const uint32_t *piece_first,
+                                            uint32_t F1, uint32_t k) {
+  uint32_t lo = 0, hi = F1;  // last p1 with piece_first[p1] <= k
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (piece_first[mid] <= k) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Histogram of piece k on the second-pass bits.
+template <typename K>
+__global__ void __launch_bounds__(512)
+    piece_histogram_kernel(const Tuple<K> *__restrict__ rel1,
+                           const uint64_t *__restrict__ off1, uint32_t C1,
+                           uint32_t F1, uint32_t F2, uint64_t mask2,
+                           uint32_t ign2, Pass2Plan pl) {
+  extern __shared__ uint32_t hist[];
+  const uint32_t k = blockIdx.x;
+  const uint32_t total = pl.piece_first[F1];
+  if (k >= total) return;
+  const uint32_t p1 = find_p1(pl.piece_first, F1, k);
+  const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
+  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  for (uint32_t i = threadIdx.x; i < F2; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const uint64_t *rp = pl.reg_pre + (uint64_t)p1 * (C1 + 1);
+  for (uint32_t c = 0; c < C1; ++c) {
+    const uint64_t rb = rp[c], re = rp[c + 1];
+    const uint64_t lo = max(rb, s0), hi = min(re, s1);
+    if (lo >= hi) continue;
+    const uint64_t phys = off1[(uint64_t)c * F1 + p1] + (lo - rb);
+    const uint64_t cnt = hi - lo;
+    for (uint64_t base = 0; base < cnt; base += blockDim.x) {
+      const uint64_t i = base + threadIdx.x;
+      const bool act = i < cnt;
+      const K key = act ? __ldcs(&rel1[phys + i].key) : K(0);
+      warp_aggregated_count(hist, key_to_partition(key, mask2, ign2), act);
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < F2; i += blockDim.x)
+    pl.hist[(uint64_t)k * F2 + i] = hist[i];
+}
+
+// Output offsets per (p1, p2) and per-piece cursors; one CTA per p1.
+__global__ void __launch_bounds__(1024)
+    pass2_cursor_kernel(uint32_t F1, uint32_t F2, Pass2Plan pl) {
+  extern __shared__ uint32_t tot[];  // [F2] + 33
+  uint32_t *scan_tmp = tot + F2;
+  const uint32_t p1 = blockIdx.x;
+  const uint32_t kb = pl.piece_first[p1], ke = pl.piece_first[p1 + 1];
+  for (uint32_t p2 = threadIdx.x; p2 < F2; p2 += blockDim.x) {
+    uint32_t t = 0;
+    for (uint32_t k = kb; k < ke; ++k) t += pl.hist[(uint64_t)k * F2 + p2];
+    tot[p2] = t;
+  }
+  __syncthreads();
+  block_exclusive_scan_u32(tot, F2, scan_tmp);
+  const uint64_t base = pl.p1_base[p1];
+  for (uint32_t p2 = threadIdx.x; p2 < F2; p2 += blockDim.x) {
+    uint64_t run = base + tot[p2];
+    pl.off2[(uint64_t)p1 * F2 + p2] = run;
+    for (uint32_t k = kb; k < ke; ++k) {
+      pl.cursor[(uint64_t)k * F2 + p2] = run;
+      run += pl.hist[(uint64_t)k * F2 + p2];
+    }
+  }
+  if (p1 + 1 == F1 && threadIdx.x == 0) pl.off2[(uint64_t)F1 * F2] = pl.p1_base[F1];
+}
+
+// Scatter of piece k into the (p1, p2)-ordered output.
+template <typename K>
+__global__ void __launch_bounds__(TileCfg<K>::kThreads, 1)
+    pass2_scatter_kernel(const Tuple<K> *__restrict__ rel1,
+                         const uint64_t *__restrict__ off1, uint32_t C1,
+                         uint32_t F1, uint32_t F2, uint64_t mask2,
+                         uint32_t ign2, Pass2Plan pl,
+                         Tuple<K> *__restrict__ rel2, uint64_t rel2_len,
+                         int *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Tuple<K> *staged = reinterpret_cast<Tuple<K> *>(smem_raw);
+  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + tile_tuples<K>());
+  uint32_t *cur = toff + F2 + 1;
+  uint32_t *scan_tmp = cur + F2;
+  const uint32_t k = blockIdx.x;
+  const uint32_t total = pl.piece_first[F1];
+  if (k >= total) return;
+  const uint32_t p1 = find_p1(pl.piece_first, F1, k);
+  const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
+  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  const uint64_t *cp = pl.cursor + (uint64_t)k * F2;
+  const uint64_t base = cp[0];
+  for (uint32_t p = threadIdx.x; p < F2; p += blockDim.x) {
+    cur[p] = (uint32_t)(cp[p] - base);
+    toff[p] = 0;
+  }
+  if (threadIdx.x == 0) toff[F2] = 0;
+  __syncthreads();
+  const uint64_t *rp = pl.reg_pre + (uint64_t)p1 * (C1 + 1);
+  TupleSource<K> src{rel1};
+  for (uint32_t c = 0; c < C1; ++c) {
+    const uint64_t rb = rp[c], re = rp[c + 1];
+    const uint64_t lo = max(rb, s0), hi = min(re, s1);
+    if (lo >= hi) continue;
+    const uint64_t phys = off1[(uint64_t)c * F1 + p1] + (lo - rb);
+    tile_scatter_range<K>(src, phys, phys + (hi - lo), F2, mask2, ign2, cur,
+                          toff, scan_tmp, staged, rel2, base, rel2_len, status);
+  }
+}
+
+__global__ void __launch_bounds__(1024)
+    finish_result_kernel(const int64_t *__restrict__ sums, uint64_t n,
+                         const uint64_t *count, fi_join_result *result) {
+  __shared__ uint64_t tmp[32];
+  uint64_t s = 0;
+  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) s += (uint64_t)sums[i];
+  s = block_reduce_u64(s, tmp);
+  if (threadIdx.x == 0) {
+    result->sum = (int64_t)s;
+    result->count = *count;
+  }
+}
+
+}  // namespace fi
+
+using namespace fi;
+
+struct fi_radix_join_engine {
+  uint64_t max_build, max_probe;
+  uint32_t tuple_bytes;
+  int32_t bits1, bits2;  // bits2 < 0: single pass
+  fi_hashing_scheme scheme;
+  uint32_t sm_count, C1, F1, F2, max_pieces;
+  DevBuf rel1[2], off1[2], loc1[2], rel2[2];
+  DevBuf reg_pre[2], p1_base[2], piece_first[2], piece_tmp[2], hist2[2],
+      cursor2[2], off2[2];
+  DevBuf hist_scratch, tile_state, counters, status;
+  DevBuf join_items, join_counters, join_tiles, join_sums, join_count;
+  DevBuf in_cols[4];  // device copies of host input (run_host)
+  uint64_t workspace = 0;
+  cudaEvent_t events[FI_ENGINE_PHASE_EVENTS] = {};
+  bool record = false;
+  uint32_t launches = 0;
+
+  void mark(int i, cudaStream_t st) {
+    if (record) cudaEventRecord(events[i], st);
+  }
+
+  int alloc(DevBuf &b, size_t bytes, bool zero = false) {
+    int rc = b.reserve(bytes, zero);
+    if (rc == FI_OK) workspace += bytes;
+    return rc;
+  }
+  HistScratch hs() {
+    return HistScratch{(uint32_t *)hist_scratch.ptr, (uint64_t *)tile_state.ptr,
+                       (uint32_t *)counters.ptr, (int *)status.ptr};
+  }
+  Pass2Plan plan(int r) {
+    return Pass2Plan{(uint64_t *)reg_pre[r].ptr, (uint64_t *)p1_base[r].ptr,
+                     (uint32_t *)piece_first[r].ptr, (uint32_t *)hist2[r].ptr,
+                     (uint64_t *)cursor2[r].ptr, (uint64_t *)off2[r].ptr};
+  }
+  void release_all() {
+    for (int r = 0; r < 2; ++r) {
+      rel1[r].release(); off1[r].release(); loc1[r].release(); rel2[r].release();
+      reg_pre[r].release(); p1_base[r].release(); piece_first[r].release();
+      piece_tmp[r].release(); hist2[r].release(); cursor2[r].release();
+      off2[r].release();
+    }
+    hist_scratch.release(); tile_state.release(); counters.release();
+    status.release(); join_items.release(); join_counters.release();
+    join_tiles.release(); join_sums.release(); join_count.release();
+    for (auto &b : in_cols) b.release();
+  }
+};
+
+extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
+                                        uint64_t max_probe_len,
+                                        uint32_t tuple_bytes,
+                                        fi_radix_bits radix_bits,
+                                        fi_hashing_scheme hashing_scheme,
+                                        fi_radix_join_engine **out) {
+  if (!out) return set_error(FI_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (tuple_bytes != 8 && tuple_bytes != 16)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "tuple_bytes must be 8 or 16");
+  if (hashing_scheme != FI_HASHING_PERFECT &&
+      hashing_scheme != FI_HASHING_BUCKET_CHAINING)
+    return set_error(FI_ERR_UNSUPPORTED,
+                     "the radix join supports Perfect and BucketChaining");
+  const int32_t b1 = radix_bits.pass_bits[0], b2 = radix_bits.pass_bits[1];
+  if (b1 < 0 || b1 > (int32_t)kMaxHistBits || b1 > (int32_t)kMaxTileBits ||
+      b2 > 10 || radix_bits.pass_bits[2] >= 0)
+    return set_error(FI_ERR_UNSUPPORTED,
+                     "the engine supports one or two passes with at most 14 "
+                     "first-pass and 10 second-pass bits");
+  if (b2 >= 0 && b1 + b2 > 24)
+    return set_error(FI_ERR_UNSUPPORTED, "at most 24 radix bits in total");
+  auto *e = new fi_radix_join_engine();
+  e->max_build = max_build_len;
+  e->max_probe = max_probe_len;
+  e->tuple_bytes = tuple_bytes;
+  e->bits1 = b1;
+  e->bits2 = b2;
+  e->scheme = hashing_scheme;
+  e->sm_count = (uint32_t)device_sm_count();
+  e->C1 = e->sm_count;
+  e->F1 = 1u << b1;
+  e->F2 = b2 >= 0 ? (1u << b2) : 1u;
+  const uint64_t maxn = std::max(max_build_len, max_probe_len);
+  e->max_pieces = (uint32_t)((maxn + kPieceTuples - 1) / kPieceTuples + e->F1);
+  const uint64_t pad = kPaddingBytes / tuple_bytes;
+  const uint32_t pass1_chunks = b2 >= 0 ? e->C1 : 1;
+  int rc = FI_OK;
+  const uint64_t lens[2] = {max_build_len, max_probe_len};
+  for (int r = 0; r < 2 && !rc; ++r) {
+    rc = e->alloc(e->rel1[r], (lens[r] + (uint64_t)pass1_chunks * e->F1 * pad) *
+                                  tuple_bytes);
+    if (!rc) rc = e->alloc(e->off1[r], (size_t)e->C1 * e->F1 * 8);
+    if (!rc && b2 < 0) rc = e->alloc(e->loc1[r], (size_t)e->C1 * e->F1 * 8);
+    if (!rc && b2 >= 0) {
+      rc = e->alloc(e->rel2[r], std::max<uint64_t>(lens[r], 1) * tuple_bytes);
+      if (!rc) rc = e->alloc(e->reg_pre[r], (size_t)e->F1 * (e->C1 + 1) * 8);
+      if (!rc) rc = e->alloc(e->p1_base[r], (size_t)(e->F1 + 1) * 8);
+      if (!rc) rc = e->alloc(e->piece_first[r], (size_t)(e->F1 + 1) * 4);
+      if (!rc) rc = e->alloc(e->piece_tmp[r], (size_t)(e->F1 + 1) * 8);
+      if (!rc) rc = e->alloc(e->hist2[r], (size_t)e->max_pieces * e->F2 * 4);
+      if (!rc) rc = e->alloc(e->cursor2[r], (size_t)e->max_pieces * e->F2 * 8);
+      if (!rc) rc = e->alloc(e->off2[r], ((size_t)e->F1 * e->F2 + 1) * 8);
+    }
+  }
+  const uint32_t Fj = e->F1 * e->F2;
+  if (!rc) rc = e->alloc(e->hist_scratch, (size_t)e->C1 * e->F1 * 4, true);
+  if (!rc) rc = e->alloc(e->tile_state, ((size_t)e->F1 / kScanTile + 2) * 8, true);
+  if (!rc) rc = e->alloc(e->counters, 16, true);
+  if (!rc) rc = e->alloc(e->status, 16, true);
+  if (!rc) rc = e->alloc(e->join_items, ((size_t)Fj + 1) * 4);
+  if (!rc) rc = e->alloc(e->join_counters, 16, true);
+  if (!rc) rc = e->alloc(e->join_tiles, ((size_t)Fj / 1024 + 2) * 8, true);
+  if (!rc) rc = e->alloc(e->join_sums, (size_t)e->sm_count * kJoinBlock * 8);
+  if (!rc) rc = e->alloc(e->join_count, 16);
+  if (rc) {
+    e->release_all();
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return FI_OK;
+}
+
+extern "C" void fi_radix_join_engine_free(fi_radix_join_engine *e) {
+  if (!e) return;
+  e->release_all();
+  delete e;
+}
+
+extern "C" uint64_t fi_radix_join_engine_workspace_bytes(
+    const fi_radix_join_engine *e) {
+  return e ? e->workspace : 0;
+}
+
+extern "C" int fi_radix_join_engine_status(fi_radix_join_engine *e) {
+  if (!e) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  return read_and_clear_status(e->status);
+}
+
+#define FI_CK(expr, what)                                                      \
+  do {                                                                         \
+    cudaError_t e_ = (expr);                                                   \
+    if (e_ != cudaSuccess) return cuda_error(e_, what);                        \
+  } while (0)
+
+template <typename K>
+static int engine_run(fi_radix_join_engine *e, const K *bk, const K *bp,
+                      uint64_t bn, const K *pk, const K *pp, uint64_t pn,
+                      fi_join_result *result, cudaStream_t st) {
+  if (!e || !result) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  if (e->tuple_bytes != 2 * sizeof(K))
+    return set_error(FI_ERR_INVALID_ARGUMENT, "engine built for another tuple type");
+  if (bn > e->max_build || pn > e->max_probe)
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "relation larger than the engine's workspace");
+  const uint32_t C1 = e->C1, F1 = e->F1, F2 = e->F2;
+  const uint32_t b1 = (uint32_t)e->bits1;
+  const uint32_t pad = kPaddingBytes / e->tuple_bytes;
+  const K *keys[2] = {bk, pk}, *pays[2] = {bp, pp};
+  const uint64_t lens[2] = {bn, pn};
+  const int scheme = e->scheme == FI_HASHING_PERFECT ? 0 : 2;
+  for (int r = 0; r < 2; ++r)
+    if ((uint64_t)(lens[r] + C1 - 1) / C1 >= 0xffffffffull)
+      return set_error(FI_ERR_INTEGER_OVERFLOW, "relation too large");
+
+  FI_CK(cudaMemsetAsync(e->join_sums.ptr, 0, e->join_sums.size, st), "memset");
+  FI_CK(cudaMemsetAsync(e->join_count.ptr, 0, 8, st), "memset");
+  JoinScratch js{(uint32_t *)e->join_items.ptr, (uint32_t *)e->join_counters.ptr,
+                 (uint64_t *)e->join_tiles.ptr,
+                 (uint32_t *)e->join_counters.ptr + 1, (int *)e->status.ptr};
+  const uint32_t hist_launches = hist_splits(C1, e->sm_count) == 1 ? 1u : 2u;
+  e->launches = 0;
+  e->mark(0, st);
+
+  if (e->bits2 < 0) {
+    // single pass: Contiguous layout (one chunk) for the join
+    uint64_t padded[2];
+    for (int r = 0; r < 2; ++r) {
+      padded[r] = lens[r] + (uint64_t)F1 * pad;
+      FI_CK(launch_contiguous_prefix_sum<K>(
+                keys[r], nullptr, lens[r], C1, b1, 0, pad, nullptr, nullptr,
+                (uint64_t *)e->off1[r].ptr, (uint64_t *)e->loc1[r].ptr, e->hs(),
+                e->sm_count, st),
+            "prefix sum");
+      e->mark(1 + 4 * r, st);
+      FI_CK(launch_partition<K>(keys[r], pays[r], lens[r], C1, b1, 0,
+                                (const uint64_t *)e->loc1[r].ptr,
+                                e->rel1[r].ptr, padded[r], false,
+                                (int *)e->status.ptr, st),
+            "partition");
+      e->mark(2 + 4 * r, st);
+      e->mark(3 + 4 * r, st);
+      e->mark(4 + 4 * r, st);
+      e->launches += 3;
+    }
+    FI_CK(launch_radix_join<K>(e->rel1[0].ptr, (const uint64_t *)e->off1[0].ptr,
+                               padded[0], pad, e->rel1[1].ptr,
+                               (const uint64_t *)e->off1[1].ptr, padded[1], pad,
+                               F1, b1, scheme, e->sm_count, kJoinBlock,
+                               (int64_t *)e->join_sums.ptr,
+                               (uint64_t *)e->join_count.ptr, js, e->sm_count,
+                               st),
+          "join");
+  } else {
+    const uint32_t b2 = (uint32_t)e->bits2;
+    const uint64_t mask2 = (uint64_t)(F2 - 1u) << b1;
+    for (int r = 0; r < 2; ++r) {
+      const uint64_t padded1 = lens[r] + (uint64_t)C1 * F1 * pad;
+      FI_CK(launch_chunked_prefix_sum<K>(keys[r], lens[r], C1, b1, 0, pad,
+                                         (uint64_t *)e->off1[r].ptr, e->hs(),
+                                         e->sm_count, st),
+            "pass-1 prefix sum");
+      e->mark(1 + 4 * r, st);
+      FI_CK(launch_partition<K>(keys[r], pays[r], lens[r], C1, b1, 0,
+                                (const uint64_t *)e->off1[r].ptr,
+                                e->rel1[r].ptr, padded1, false,
+                                (int *)e->status.ptr, st),
+            "pass-1 partition");
+      e->mark(2 + 4 * r, st);
+      Pass2Plan pl = e->plan(r);
+      pass2_plan_kernel<<<1, 1024, 0, st>>>((const uint64_t *)e->off1[r].ptr, C1,
+                                            F1, padded1, pad, pl,
+                                            (uint64_t *)e->piece_tmp[r].ptr);
+      FI_CK(cudaGetLastError(), "pass-2 plan");
+      piece_histogram_kernel<K><<<e->max_pieces, 512, F2 * 4, st>>>(
+          (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
+          C1, F1, F2, mask2, b1, pl);
+      FI_CK(cudaGetLastError(), "pass-2 histogram");
+      const size_t csm = (size_t)(F2 + 33) * 4;
+      pass2_cursor_kernel<<<F1, 1024, csm, st>>>(F1, F2, pl);
+      FI_CK(cudaGetLastError(), "pass-2 cursors");
+      e->mark(3 + 4 * r, st);
+      const size_t ssm = tile_scatter_smem<K>(F2);
+      FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_kernel<K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ssm),
+            "smem attribute");
+      pass2_scatter_kernel<K><<<e->max_pieces, TileCfg<K>::kThreads, ssm, st>>>(
+          (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
+          C1, F1, F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, lens[r],
+          (int *)e->status.ptr);
+      FI_CK(cudaGetLastError(), "pass-2 scatter");
+      e->mark(4 + 4 * r, st);
+      e->launches += hist_launches + 1 + 4;
+    }
+    FI_CK(launch_radix_join<K>(e->rel2[0].ptr, (const uint64_t *)e->off2[0].ptr,
+                               lens[0], 0, e->rel2[1].ptr,
+                               (const uint64_t *)e->off2[1].ptr, lens[1], 0,
+                               F1 * F2, b1 + b2, scheme, e->sm_count,
+                               kJoinBlock, (int64_t *)e->join_sums.ptr,
+                               (uint64_t *)e->join_count.ptr, js, e->sm_count,
+                               st),
+          "join");
+  }
+  e->mark(9, st);
+  finish_result_kernel<<<1, 1024, 0, st>>>(
+      (const int64_t *)e->join_sums.ptr, (uint64_t)e->sm_count * kJoinBlock,
+      (const uint64_t *)e->join_count.ptr, result);
+  e->launches += 3;  // join plan, join, result
+  FI_CK(cudaGetLastError(), "result");
+  e->mark(10, st);
+  return FI_OK;
+}
+
+extern "C" int fi_radix_join_engine_set_events(fi_radix_join_engine *e,
+                                               void **events,
+                                               uint32_t n_events) {
+  if (!e) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  if (!events) {
+    e->record = false;
+    return FI_OK;
+  }
+  if (n_events < FI_ENGINE_PHASE_EVENTS)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "need %d events",
+                     FI_ENGINE_PHASE_EVENTS);
+  for (int i = 0; i < FI_ENGINE_PHASE_EVENTS; ++i)
+    e->events[i] = (cudaEvent_t)events[i];
+  e->record = true;
+  return FI_OK;
+}
+
+extern "C" uint32_t fi_radix_join_engine_last_launches(
+    const fi_radix_join_engine *e) {
+  return e ? e->launches : 0;
+}
+
+extern "C" int fi_radix_join_engine_run_int32(
+    fi_radix_join_engine *e, const int32_t *build_key, const int32_t *build_pay,
+    uint64_t build_len, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_run<int32_t>(e, build_key, build_pay, build_len, probe_key,
+                             probe_pay, probe_len, result, (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_run_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_run<int64_t>(e, build_key, build_pay, build_len, probe_key,
+                             probe_pay, probe_len, result, (cudaStream_t)stream);
+}
+
+extern "C" int fi_radix_join_engine_run_host_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  if (!e || !result) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t *src[4] = {build_key, build_pay, probe_key, probe_pay};
+  const uint64_t lens[4] = {build_len, build_len, probe_len, probe_len};
+  for (int i = 0; i < 4; ++i) {
+    int rc = e->in_cols[i].reserve(std::max<uint64_t>(lens[i], 1) * 8, false);
+    if (rc) return rc;
+    FI_CK(cudaMemcpyAsync(e->in_cols[i].ptr, src[i], lens[i] * 8,
+                          cudaMemcpyHostToDevice, st),
+          "host-to-device copy");
+  }
+  DevBuf dres;
+  int rc = dres.reserve(sizeof(fi_join_result), false);
+  if (rc) return rc;
+  rc = engine_run<int64_t>(e, (const int64_t *)e->in_cols[0].ptr,
+                           (const int64_t *)e->in_cols[1].ptr, build_len,
+                           (const int64_t *)e->in_cols[2].ptr,
+                           (const int64_t *)e->in_cols[3].ptr, probe_len,
+                           (fi_join_result *)dres.ptr, st);
+  if (rc == FI_OK) {
+    cudaError_t ce = cudaMemcpyAsync(result, dres.ptr, sizeof(fi_join_result),
+                                     cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = cuda_error(ce, "result copy");
+  }
+  dres.release();
+  return rc;
+}

@@ -1,0 +1,220 @@
+// Radix-partition scatter kernels (sm_100a).
+//
+// Replaces the reference's scatter variants NC, LASWWC, SSWWCv2, SSWWCv2G and
+// HSSWWCv4 (sql-ops/cudautils/radix_partition.cu:472-1477).  Every variant
+// writes tuple (key, payload) of chunk c with partition p into the slots
+// [cursors[c*F+p], ...) of the partitioned relation, so the per-(chunk,
+// partition) tuple multisets equal the reference's; padding is never written.
+//
+// B200 design of the write-combining scatter ("tile scatter"):
+//  * One CTA owns one chunk (the Chunked layout's unit) and walks it in tiles
+//    of kTile tuples.  The next tile's keys and payloads are loaded into
+//    registers (evict-first) while the current tile is processed, so HBM
+//    reads stay in flight across the block barriers.
+//  * Each tile is counting-sorted by partition in shared memory: a
+//    warp-aggregated rank (match.any + one shared atomic per distinct
+//    partition per warp) and a block scan of the tile histogram give every
+//    tuple its slot in a staging buffer.
+//  * The staged tile is written out in partition runs: consecutive threads
+//    write consecutive tuples of a run, so a warp store covers a few
+//    contiguous 128-byte segments instead of 32 scattered ones.  Partially
+//    written lines are completed by the next tiles while they sit in the
+//    126 MB L2, which therefore acts as the write-combining buffer that the
+//    reference keeps in shared memory and flushes under warp locks.
+//  * No device-side waits: the only synchronisation is __syncthreads.
+//  * Every store is bounds-checked against the relation's length.
+#include "common.cuh"
+#include "kernels.h"
+#include "tile_scatter.cuh"
+
+namespace fi {
+
+// One CTA per canonical chunk of column input.
+template <typename K>
+__global__ void __launch_bounds__(TileCfg<K>::kThreads, 1)
+    tile_scatter_kernel(const K *__restrict__ keys, const K *__restrict__ pays,
+                        uint64_t len, uint64_t clen, uint32_t chunks,
+                        uint32_t radix_bits, uint32_t ignore_bits,
+                        const uint64_t *__restrict__ cursors,
+                        Tuple<K> *__restrict__ out, uint64_t out_len,
+                        int *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  Tuple<K> *staged = reinterpret_cast<Tuple<K> *>(smem_raw);
+  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + tile_tuples<K>());
+  uint32_t *cur = toff + F + 1;
+  uint32_t *scan_tmp = cur + F;
+
+  const uint32_t c = blockIdx.x;
+  const uint64_t cb = clen * c, ce = (c + 1 == chunks) ? len : cb + clen;
+  const uint64_t base = cursors[(uint64_t)c * F];
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x) {
+    cur[p] = (uint32_t)(cursors[(uint64_t)c * F + p] - base);
+    toff[p] = 0;
+  }
+  if (threadIdx.x == 0) toff[F] = 0;
+  __syncthreads();
+  ColumnSource<K> src{keys, pays};
+  tile_scatter_range<K>(src, cb, ce, F, mask,
+                        ignore_bits, cur, toff, scan_tmp, staged, out, base,
+                        out_len, status);
+}
+
+// Non-caching scatter: one shared-memory atomic per tuple and a direct
+// store (the reference's NC, radix_partition.cu:472-525).
+template <typename K>
+__global__ void __launch_bounds__(1024)
+    nc_scatter_kernel(const K *__restrict__ keys, const K *__restrict__ pays,
+                      uint64_t len, uint64_t clen, uint32_t chunks,
+                      uint32_t radix_bits, uint32_t ignore_bits,
+                      const uint64_t *__restrict__ cursors,
+                      Tuple<K> *__restrict__ out, uint64_t out_len,
+                      int *status) {
+  extern __shared__ uint32_t cur[];
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  const uint32_t c = blockIdx.x;
+  const uint64_t cb = clen * c, ce = (c + 1 == chunks) ? len : cb + clen;
+  const uint64_t base = cursors[(uint64_t)c * F];
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    cur[p] = (uint32_t)(cursors[(uint64_t)c * F + p] - base);
+  __syncthreads();
+  for (uint64_t i = cb + threadIdx.x; i < ce; i += blockDim.x) {
+    const K k = load_cs(keys + i), v = load_cs(pays + i);
+    const uint32_t p = key_to_partition(k, mask, ignore_bits);
+    const uint64_t dst = base + atomicAdd(&cur[p], 1u);
+    if (dst < out_len)
+      store_tuple(out + dst, Tuple<K>{k, v});
+    else
+      record_error(status, kDevErrCapacity);
+  }
+}
+
+// Level 2 of the hierarchical scatter: CTA per (chunk, high bucket) region
+// of the level-1 buffer; scatters it by the low bits into the final slots.
+template <typename K>
+__global__ void __launch_bounds__(TileCfg<K>::kThreads, 1)
+    hierarchical_level2_kernel(const Tuple<K> *__restrict__ tmp,
+                               const uint64_t *__restrict__ tmp_cursors,
+                               uint64_t len, uint32_t chunks, uint32_t hi_bits,
+                               uint32_t lo_bits, uint32_t ignore_bits,
+                               const uint64_t *__restrict__ cursors,
+                               Tuple<K> *__restrict__ out, uint64_t out_len,
+                               int *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t FH = 1u << hi_bits, FL = 1u << lo_bits, F = FH * FL;
+  const uint64_t mask = static_cast<uint64_t>(FL - 1u) << ignore_bits;
+  Tuple<K> *staged = reinterpret_cast<Tuple<K> *>(smem_raw);
+  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + tile_tuples<K>());
+  uint32_t *cur = toff + FL + 1;
+  uint32_t *scan_tmp = cur + FL;
+
+  const uint32_t item = blockIdx.x;  // c * FH + h
+  const uint32_t c = item / FH, h = item % FH;
+  const uint64_t begin = tmp_cursors[item];
+  const uint64_t end = (item + 1 < chunks * FH) ? tmp_cursors[item + 1] : len;
+  if (begin >= end) return;
+  const uint64_t *cp = cursors + (uint64_t)c * F + (uint64_t)h * FL;
+  const uint64_t base = cp[0];
+  for (uint32_t p = threadIdx.x; p < FL; p += blockDim.x) {
+    cur[p] = (uint32_t)(cp[p] - base);
+    toff[p] = 0;
+  }
+  if (threadIdx.x == 0) toff[FL] = 0;
+  __syncthreads();
+  TupleSource<K> src{tmp};
+  tile_scatter_range<K>(src, begin, end, FL, mask, ignore_bits,
+                        cur, toff, scan_tmp, staged, out, base, out_len,
+                        status);
+}
+
+uint32_t hierarchical_hi_bits(uint32_t radix_bits) { return (radix_bits + 1) / 2; }
+
+template <typename K>
+static cudaError_t launch_tile(const K *keys, const K *pays, uint64_t len,
+                               uint32_t chunks, uint32_t radix_bits,
+                               uint32_t ignore_bits, const uint64_t *cursors,
+                               void *out, uint64_t out_len, int *status,
+                               cudaStream_t stream) {
+  const uint32_t F = 1u << radix_bits;
+  constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+  const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
+  const size_t sm = tile_scatter_smem<K>(F);
+  cudaError_t e = cudaFuncSetAttribute(
+      (const void *)tile_scatter_kernel<K>,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  tile_scatter_kernel<K><<<chunks, TileCfg<K>::kThreads, sm, stream>>>(
+      keys, pays, len, clen, chunks, radix_bits, ignore_bits, cursors,
+      reinterpret_cast<Tuple<K> *>(out), out_len, status);
+  return cudaGetLastError();
+}
+
+template <typename K>
+cudaError_t launch_partition(const K *keys, const K *pays, uint64_t len,
+                             uint32_t chunks, uint32_t radix_bits,
+                             uint32_t ignore_bits, const uint64_t *cursors,
+                             void *out, uint64_t out_len, bool nc, int *status,
+                             cudaStream_t stream) {
+  const uint32_t F = 1u << radix_bits;
+  if (nc) {
+    constexpr uint64_t kAlignMask =
+        ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+    const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
+    const size_t sm = (size_t)F * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(
+        (const void *)nc_scatter_kernel<K>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    nc_scatter_kernel<K><<<chunks, 1024, sm, stream>>>(
+        keys, pays, len, clen, chunks, radix_bits, ignore_bits, cursors,
+        reinterpret_cast<Tuple<K> *>(out), out_len, status);
+    return cudaGetLastError();
+  }
+  return launch_tile<K>(keys, pays, len, chunks, radix_bits, ignore_bits,
+                        cursors, out, out_len, status, stream);
+}
+
+template <typename K>
+cudaError_t launch_partition_hierarchical(
+    const K *keys, const K *pays, uint64_t len, uint32_t chunks,
+    uint32_t radix_bits, uint32_t ignore_bits, const uint64_t *cursors,
+    void *out, uint64_t out_len, void *tmp, uint64_t *tmp_cursors,
+    HistScratch s, uint32_t sm_count, cudaStream_t stream) {
+  const uint32_t hi = hierarchical_hi_bits(radix_bits), lo = radix_bits - hi;
+  // level-1 layout: same canonical chunks, partitions by the high bits, no
+  // padding
+  cudaError_t e = launch_chunked_prefix_sum<K>(keys, len, chunks, hi,
+                                               ignore_bits + lo, 0u,
+                                               tmp_cursors, s, sm_count, stream);
+  if (e != cudaSuccess) return e;
+  e = launch_tile<K>(keys, pays, len, chunks, hi, ignore_bits + lo,
+                     tmp_cursors, tmp, len, s.status, stream);
+  if (e != cudaSuccess) return e;
+  const size_t sm = tile_scatter_smem<K>(1u << lo);
+  e = cudaFuncSetAttribute((const void *)hierarchical_level2_kernel<K>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm);
+  if (e != cudaSuccess) return e;
+  hierarchical_level2_kernel<K>
+      <<<chunks << hi, TileCfg<K>::kThreads, sm, stream>>>(
+          reinterpret_cast<const Tuple<K> *>(tmp), tmp_cursors, len, chunks,
+          hi, lo, ignore_bits, cursors, reinterpret_cast<Tuple<K> *>(out),
+          out_len, s.status);
+  return cudaGetLastError();
+}
+
+#define FI_INSTANTIATE_PARTITION(K)                                            \
+  template cudaError_t launch_partition<K>(                                    \
+      const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t,            \
+      const uint64_t *, void *, uint64_t, bool, int *, cudaStream_t);          \
+  template cudaError_t launch_partition_hierarchical<K>(                       \
+      const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t,            \
+      const uint64_t *, void *, uint64_t, void *, uint64_t *, HistScratch,     \
+      uint32_t, cudaStream_t);
+
+FI_INSTANTIATE_PARTITION(int32_t)
+FI_INSTANTIATE_PARTITION(int64_t)
+
+}  // namespace fi

@@ -1,0 +1,482 @@
+// Histogram and prefix-sum kernels of the radix partitioner (sm_100a).
+//
+// Replaces gpu_chunked_prefix_sum, gpu_contiguous_prefix_sum,
+// gpu_contiguous_prefix_sum_and_copy_with_payload and
+// gpu_contiguous_prefix_sum_and_transform of the reference
+// (sql-ops/cudautils/radix_partition.cu:40-467) with the same outputs.
+//
+// Design (B200):
+//  * Histogram: every chunk is shared by `splits` CTAs so that the grid fills
+//    all 148 SMs even with few chunks.  Keys stream in with 16-byte
+//    evict-first vector loads; counts go to a shared-memory histogram through
+//    warp-aggregated atomics (match.any), which keeps Zipf-skewed keys from
+//    serialising on one counter.  A chunk owned by a single CTA is scanned in
+//    place and its offsets written directly (one launch); otherwise the CTAs
+//    add their counts into a global per-chunk histogram and a second kernel
+//    scans it.
+//  * Contiguous offsets: instead of the reference's cooperative launch with
+//    three grid-wide barriers, a second kernel scans the (partition, chunk)
+//    counts with a single-pass decoupled look-back over tiles of partitions
+//    (Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
+//    Look-back", 2016): tile ids are taken from an atomic counter so a tile
+//    only waits on tiles that are already running, and every wait is bounded.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fi {
+
+constexpr uint32_t kHistThreads = 512;
+constexpr uint32_t kHistUnroll = 4;
+constexpr uint32_t kScanThreads = kScanTile;  // one partition per thread
+
+template <typename K>
+struct Vec16;
+template <>
+struct Vec16<int64_t> {
+  using type = longlong2;
+  static constexpr uint32_t n = 2;
+  __device__ static int64_t get(const longlong2 &v, uint32_t i) {
+    return i == 0 ? v.x : v.y;
+  }
+};
+template <>
+struct Vec16<int32_t> {
+  using type = int4;
+  static constexpr uint32_t n = 4;
+  __device__ static int32_t get(const int4 &v, uint32_t i) {
+    return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+  }
+};
+
+// Calls f(key, active) for keys[begin, end) in warp-uniform iterations, so
+// that f may use warp intrinsics.  16-byte vector loads when the column is
+// 16-byte aligned; scalar loads for the ragged head and tail.
+template <typename K, typename Fn>
+__device__ __forceinline__ void for_each_key(const K *__restrict__ keys,
+                                             uint64_t begin, uint64_t end,
+                                             Fn &&f) {
+  using VT = Vec16<K>;
+  using V = typename VT::type;
+  constexpr uint32_t kVec = VT::n;
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  uint64_t vb = (begin + kVec - 1) / kVec, ve = end / kVec;
+  const bool aligned = (reinterpret_cast<uintptr_t>(keys) % 16) == 0;
+  if (!aligned || vb >= ve) {
+    for (uint64_t base = begin; base < end; base += nt) {
+      uint64_t i = base + tid;
+      bool act = i < end;
+      f(act ? load_cs(keys + i) : K(0), act);
+    }
+    return;
+  }
+  {  // head: fewer than kVec elements
+    uint64_t i = begin + tid;
+    bool act = i < vb * kVec;
+    f(act ? load_cs(keys + i) : K(0), act);
+  }
+  const V *vk = reinterpret_cast<const V *>(keys);
+  for (uint64_t base = vb; base < ve; base += (uint64_t)nt * kHistUnroll) {
+    V v[kHistUnroll];
+    bool act[kHistUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kHistUnroll; ++u) {
+      uint64_t idx = base + (uint64_t)u * nt + tid;
+      act[u] = idx < ve;
+      if (act[u]) v[u] = __ldcs(vk + idx);
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kHistUnroll; ++u)
+#pragma unroll
+      for (uint32_t e = 0; e < kVec; ++e)
+        f(act[u] ? VT::get(v[u], e) : K(0), act[u]);
+  }
+  {  // tail
+    uint64_t i = ve * kVec + tid;
+    bool act = i < end;
+    f(act ? load_cs(keys + i) : K(0), act);
+  }
+}
+
+// Sub-range [sb, se) of chunk c handled by split s (16-byte aligned starts).
+template <typename K>
+__device__ __forceinline__ void split_range(uint64_t len, uint64_t clen,
+                                            uint32_t chunks, uint32_t c,
+                                            uint32_t splits, uint32_t s,
+                                            uint64_t &sb, uint64_t &se) {
+  constexpr uint64_t kVec = 16 / sizeof(K);
+  const uint64_t cb = clen * c;
+  const uint64_t ce = (c + 1 == chunks) ? len : cb + clen;
+  const uint64_t n = ce - cb;
+  const uint64_t per = ((n + splits - 1) / splits + kVec - 1) / kVec * kVec;
+  sb = min(ce, cb + per * s);
+  se = min(ce, sb + per);
+}
+
+// Histogram of one chunk split.  direct_offsets != nullptr: the CTA owns the
+// whole chunk (splits == 1) and writes the chunk's final offsets
+// (radix_partition.cu:83-95); otherwise it adds its counts to g_hist[c*F+p].
+// With dst_key/dst_pay the columns are copied as well.
+template <typename K>
+__global__ void __launch_bounds__(kHistThreads)
+    histogram_kernel(const K *__restrict__ keys, const K *__restrict__ pays,
+                     K *__restrict__ dst_key, K *__restrict__ dst_pay,
+                     uint64_t len, uint64_t clen, uint32_t chunks,
+                     uint32_t splits, uint32_t radix_bits,
+                     uint32_t ignore_bits, uint32_t pad,
+                     uint64_t *__restrict__ direct_offsets,
+                     uint32_t *__restrict__ g_hist) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  uint32_t *cnt = smem;
+  uint32_t *scan_tmp = smem + F;
+  const uint32_t c = blockIdx.x / splits, s = blockIdx.x % splits;
+  uint64_t sb, se;
+  split_range<K>(len, clen, chunks, c, splits, s, sb, se);
+
+  for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+
+  for_each_key(keys, sb, se, [&](K key, bool act) {
+    warp_aggregated_count(cnt, key_to_partition(key, mask, ignore_bits), act);
+  });
+
+  if (dst_key != nullptr) {
+    for (uint64_t i = sb + threadIdx.x; i < se; i += blockDim.x) {
+      dst_key[i] = keys[i];
+      dst_pay[i] = pays[i];
+    }
+  }
+  __syncthreads();
+
+  if (direct_offsets != nullptr) {
+    block_exclusive_scan_u32(cnt, F, scan_tmp);
+    const uint64_t chunk_base = (clen + (uint64_t)pad * F) * c;
+    for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+      direct_offsets[(uint64_t)c * F + p] =
+          (uint64_t)cnt[p] + chunk_base + (uint64_t)(p + 1) * pad;
+  } else {
+    for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+      if (cnt[p] != 0) atomicAdd(&g_hist[(uint64_t)c * F + p], cnt[p]);
+  }
+}
+
+// Per-chunk scan of g_hist into Chunked offsets (one CTA per chunk).
+__global__ void __launch_bounds__(1024)
+    chunked_scan_kernel(const uint32_t *__restrict__ g_hist, uint32_t F,
+                        uint64_t clen, uint32_t pad,
+                        uint64_t *__restrict__ offsets) {
+  extern __shared__ uint32_t smem[];
+  uint32_t *cnt = smem;
+  uint32_t *scan_tmp = smem + F;
+  const uint32_t c = blockIdx.x;
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    cnt[p] = g_hist[(uint64_t)c * F + p];
+  __syncthreads();
+  block_exclusive_scan_u32(cnt, F, scan_tmp);
+  const uint64_t chunk_base = (clen + (uint64_t)pad * F) * c;
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    offsets[(uint64_t)c * F + p] =
+        (uint64_t)cnt[p] + chunk_base + (uint64_t)(p + 1) * pad;
+}
+
+// ---- decoupled look-back ---------------------------------------------------
+// A tile's state word packs a 2-bit flag with a 62-bit value.
+constexpr uint64_t kFlagAggregate = 1ull << 62;
+constexpr uint64_t kFlagPrefix = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1ull;
+
+__device__ __forceinline__ void state_store(uint64_t *p, uint64_t v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v)
+               : "memory");
+}
+__device__ __forceinline__ uint64_t state_load(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];"
+               : "=l"(v)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+
+// Returns the exclusive prefix of tile t given its aggregate; thread 0 only.
+__device__ uint64_t look_back(uint64_t *tile_state, uint32_t t,
+                              uint64_t aggregate, int *status) {
+  if (t == 0) {
+    state_store(&tile_state[0], kFlagPrefix | aggregate);
+    return 0;
+  }
+  state_store(&tile_state[t], kFlagAggregate | aggregate);
+  uint64_t prefix = 0;
+  int64_t j = (int64_t)t - 1;
+  uint32_t polls = 0;
+  while (j >= 0) {
+    uint64_t s = state_load(&tile_state[j]);
+    uint64_t flag = s & ~kValueMask;
+    if (flag == 0) {
+      if (++polls > kSpinLimit) {
+        record_error(status, kDevErrTimeout);
+        break;
+      }
+      spin_pause(polls);
+      continue;
+    }
+    prefix += s & kValueMask;
+    if (flag == kFlagPrefix) break;
+    --j;
+  }
+  state_store(&tile_state[t], kFlagPrefix | (prefix + aggregate));
+  return prefix;
+}
+
+// Contiguous offsets from per-chunk histograms g_hist[b*F+p]:
+//   offsets[p]          = sum_{q<p} T[q] + (p+1)*pad,  T[q] = sum_b hist[b][q]
+//   local_offsets[b][p] = offsets[p] + sum_{b'<b} hist[b'][p]
+// (radix_partition.cu:160-198).  One partition per thread, tiles of
+// kScanTile partitions chained by decoupled look-back.
+__global__ void __launch_bounds__(kScanThreads)
+    contiguous_scan_kernel(const uint32_t *__restrict__ g_hist, uint32_t grid,
+                           uint32_t F, uint32_t pad,
+                           uint64_t *__restrict__ offsets,
+                           uint64_t *__restrict__ local_offsets,
+                           uint64_t *tile_state, uint32_t *tile_counter,
+                           int *status) {
+  __shared__ uint32_t tile_s;
+  __shared__ uint64_t prefix_s;
+  __shared__ uint64_t tmp[33];
+  if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const uint32_t t = tile_s;
+  const uint32_t p = t * kScanTile + threadIdx.x;
+  const bool act = p < F;
+  uint64_t total = 0;
+  if (act)
+    for (uint32_t b = 0; b < grid; ++b) total += g_hist[(uint64_t)b * F + p];
+  uint64_t tile_total;
+  const uint64_t excl = block_exclusive_scan_u64(total, tmp, &tile_total);
+  if (threadIdx.x == 0) prefix_s = look_back(tile_state, t, tile_total, status);
+  __syncthreads();
+  if (act) {
+    const uint64_t base = prefix_s + excl + (uint64_t)(p + 1) * pad;
+    offsets[p] = base;
+    uint64_t run = 0;
+    for (uint32_t b = 0; b < grid; ++b) {
+      local_offsets[(uint64_t)b * F + p] = base + run;
+      run += g_hist[(uint64_t)b * F + p];
+    }
+  }
+}
+
+// ---- prefix_sum_and_transform ---------------------------------------------
+// Gathers partition `pid` of every source chunk (chunk order) into columns
+// and histograms the gathered sequence per canonical chunk of `grid`
+// (radix_partition.cu:323-410).  Chunk table in shared memory; each thread
+// finds its source chunk by binary search over the chunk prefix sums.
+template <typename K>
+__global__ void __launch_bounds__(kHistThreads) transform_histogram_kernel(
+    uint32_t pid, const Tuple<K> *__restrict__ src,
+    const uint64_t *__restrict__ src_offsets, uint32_t src_chunks,
+    uint32_t src_fanout, uint64_t src_padded_len, uint32_t src_pad,
+    uint64_t dst_len, uint32_t grid, uint32_t splits, uint32_t radix_bits,
+    uint32_t ignore_bits, K *__restrict__ dst_key, K *__restrict__ dst_pay,
+    uint32_t *__restrict__ g_hist, int *status) {
+  extern __shared__ uint64_t smem64[];
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  uint64_t *ch_begin = smem64;                 // [src_chunks]
+  uint64_t *ch_pre = smem64 + src_chunks;      // [src_chunks + 1]
+  uint64_t *tmp64 = ch_pre + src_chunks + 1;   // [33]
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(tmp64 + 33);  // [F]
+
+  // chunk table: begin and length of partition pid in every source chunk
+  uint64_t local_len = 0;
+  for (uint32_t c = threadIdx.x; c < src_chunks; c += blockDim.x) {
+    uint64_t b = src_offsets[(uint64_t)c * src_fanout + pid];
+    uint64_t e = (c + 1 == src_chunks && pid + 1 == src_fanout)
+                     ? src_padded_len
+                     : src_offsets[(uint64_t)c * src_fanout + pid + 1] - src_pad;
+    ch_begin[c] = b;
+    ch_pre[c] = e - b;  // length, scanned below
+  }
+  for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t run = 0;
+    for (uint32_t c = 0; c < src_chunks; ++c) {
+      uint64_t l = ch_pre[c];
+      ch_pre[c] = run;
+      run += l;
+    }
+    ch_pre[src_chunks] = run;
+  }
+  __syncthreads();
+  (void)local_len;
+  uint64_t n = ch_pre[src_chunks];
+  if (n > dst_len) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) record_error(status, kDevErrCapacity);
+    n = dst_len;
+  }
+  constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+  const uint64_t clen = ((n + grid - 1) / grid) & kAlignMask;
+  const uint32_t b = blockIdx.x / splits, s = blockIdx.x % splits;
+  uint64_t sb, se;
+  split_range<K>(n, clen, grid, b, splits, s, sb, se);
+
+  for (uint64_t base = sb; base < se; base += blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
+    const bool act = i < se;
+    K key = 0;
+    if (act) {
+      // last chunk c with ch_pre[c] <= i
+      uint32_t lo = 0, hi = src_chunks;
+      while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ch_pre[mid] <= i) lo = mid; else hi = mid;
+      }
+      Tuple<K> t = load_tuple_cs(src + ch_begin[lo] + (i - ch_pre[lo]));
+      dst_key[i] = t.key;
+      dst_pay[i] = t.value;
+      key = t.key;
+    }
+    warp_aggregated_count(cnt, key_to_partition(key, mask, ignore_bits), act);
+  }
+  __syncthreads();
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    if (cnt[p] != 0) atomicAdd(&g_hist[(uint64_t)b * F + p], cnt[p]);
+}
+
+// ---- host launchers ---------------------------------------------------------
+uint32_t hist_splits(uint32_t chunks, uint32_t sm_count) {
+  // about two CTAs of kHistThreads per SM in total
+  uint32_t want = 2u * sm_count;
+  uint32_t s = (want + chunks - 1) / chunks;
+  return s < 1 ? 1 : s;
+}
+
+static size_t hist_smem(uint32_t F) { return (size_t)(F + 33) * sizeof(uint32_t); }
+
+template <typename K>
+static cudaError_t set_smem(const void *fn, size_t bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
+}
+
+template <typename K>
+cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
+                                      uint32_t chunks, uint32_t radix_bits,
+                                      uint32_t ignore_bits, uint32_t pad,
+                                      uint64_t *offsets, HistScratch s,
+                                      uint32_t sm_count, cudaStream_t stream) {
+  const uint32_t F = 1u << radix_bits;
+  constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+  const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
+  const uint32_t splits = hist_splits(chunks, sm_count);
+  const size_t sm = hist_smem(F);
+  cudaError_t e = set_smem<K>((const void *)histogram_kernel<K>, sm);
+  if (e != cudaSuccess) return e;
+  if (splits == 1) {
+    histogram_kernel<K><<<chunks, kHistThreads, sm, stream>>>(
+        keys, nullptr, nullptr, nullptr, len, clen, chunks, 1, radix_bits,
+        ignore_bits, pad, offsets, nullptr);
+    return cudaGetLastError();
+  }
+  e = cudaMemsetAsync(s.hist, 0, (size_t)chunks * F * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  histogram_kernel<K><<<chunks * splits, kHistThreads, sm, stream>>>(
+      keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, radix_bits,
+      ignore_bits, pad, nullptr, s.hist);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = set_smem<K>((const void *)chunked_scan_kernel, sm);
+  if (e != cudaSuccess) return e;
+  chunked_scan_kernel<<<chunks, 1024, sm, stream>>>(s.hist, F, clen, pad,
+                                                    offsets);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_contiguous_scan(uint32_t F, uint32_t grid,
+                                          uint32_t pad, uint64_t *offsets,
+                                          uint64_t *local_offsets,
+                                          HistScratch s, cudaStream_t stream) {
+  const uint32_t tiles = (F + kScanTile - 1) / kScanTile;
+  cudaError_t e =
+      cudaMemsetAsync(s.tile_state, 0, (size_t)tiles * sizeof(uint64_t), stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.tile_counter, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  contiguous_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(
+      s.hist, grid, F, pad, offsets, local_offsets, s.tile_state,
+      s.tile_counter, s.status);
+  return cudaGetLastError();
+}
+
+template <typename K>
+cudaError_t launch_contiguous_prefix_sum(const K *keys, const K *pays,
+                                         uint64_t len, uint32_t grid,
+                                         uint32_t radix_bits,
+                                         uint32_t ignore_bits, uint32_t pad,
+                                         K *dst_key, K *dst_pay,
+                                         uint64_t *offsets,
+                                         uint64_t *local_offsets,
+                                         HistScratch s, uint32_t sm_count,
+                                         cudaStream_t stream) {
+  const uint32_t F = 1u << radix_bits;
+  constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+  const uint64_t clen = ((len + grid - 1) / grid) & kAlignMask;
+  const uint32_t splits = hist_splits(grid, sm_count);
+  const size_t sm = hist_smem(F);
+  cudaError_t e = set_smem<K>((const void *)histogram_kernel<K>, sm);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.hist, 0, (size_t)grid * F * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
+      keys, pays, dst_key, dst_pay, len, clen, grid, splits, radix_bits,
+      ignore_bits, pad, nullptr, s.hist);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_contiguous_scan(F, grid, pad, offsets, local_offsets, s, stream);
+}
+
+template <typename K>
+cudaError_t launch_prefix_sum_and_transform(
+    uint32_t partition_id, const void *src_relation, const uint64_t *src_offsets,
+    uint32_t src_chunks, uint32_t src_radix_bits, uint64_t src_padded_len,
+    uint32_t src_pad, uint64_t dst_len, uint32_t grid, uint32_t radix_bits,
+    uint32_t ignore_bits, uint32_t pad, K *dst_key, K *dst_pay,
+    uint64_t *offsets, uint64_t *local_offsets, HistScratch s,
+    uint32_t sm_count, cudaStream_t stream) {
+  const uint32_t F = 1u << radix_bits;
+  const uint32_t splits = hist_splits(grid, sm_count);
+  const size_t sm = (size_t)(2 * src_chunks + 1 + 33) * sizeof(uint64_t) +
+                    (size_t)F * sizeof(uint32_t);
+  cudaError_t e =
+      set_smem<K>((const void *)transform_histogram_kernel<K>, sm);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.hist, 0, (size_t)grid * F * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  transform_histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
+      partition_id, reinterpret_cast<const Tuple<K> *>(src_relation),
+      src_offsets, src_chunks, 1u << src_radix_bits, src_padded_len, src_pad,
+      dst_len, grid, splits, radix_bits, ignore_bits, dst_key, dst_pay, s.hist,
+      s.status);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_contiguous_scan(F, grid, pad, offsets, local_offsets, s, stream);
+}
+
+#define FI_INSTANTIATE_PREFIX(K)                                               \
+  template cudaError_t launch_chunked_prefix_sum<K>(                           \
+      const K *, uint64_t, uint32_t, uint32_t, uint32_t, uint32_t, uint64_t *, \
+      HistScratch, uint32_t, cudaStream_t);                                    \
+  template cudaError_t launch_contiguous_prefix_sum<K>(                        \
+      const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t, uint32_t,  \
+      K *, K *, uint64_t *, uint64_t *, HistScratch, uint32_t, cudaStream_t);  \
+  template cudaError_t launch_prefix_sum_and_transform<K>(                     \
+      uint32_t, const void *, const uint64_t *, uint32_t, uint32_t, uint64_t,  \
+      uint32_t, uint64_t, uint32_t, uint32_t, uint32_t, uint32_t, K *, K *,    \
+      uint64_t *, uint64_t *, HistScratch, uint32_t, cudaStream_t);
+
+FI_INSTANTIATE_PREFIX(int32_t)
+FI_INSTANTIATE_PREFIX(int64_t)
+
+}  // namespace fi

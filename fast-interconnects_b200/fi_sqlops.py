@@ -1,0 +1,543 @@
+"""Python face of the B200 sql-ops operators: a ctypes binding of the C ABI in
+include/fi_sqlops.h, shaped like the reference's Rust API (sql-ops/src/...):
+
+* ``RadixBits``, ``RadixPass``, ``GpuHistogramAlgorithm``,
+  ``GpuRadixPartitionAlgorithm``, ``HashingScheme`` (partition.rs:35-134,
+  gpu_radix_partition.rs:192-293, join/hashing_scheme.rs:18-43);
+* ``PartitionOffsets`` and ``PartitionedRelation`` (partitioned_relation.rs)
+  holding torch tensors as memory;
+* ``GpuRadixPartitioner`` (gpu_radix_partition.rs:314-555), ``CudaRadixJoin``
+  (join/cuda_radix_join.rs:116-164), ``CudaHashJoin`` / ``HashTable``
+  (join/no_partitioning_join.rs:153-304);
+* ``RadixJoinEngine``: the gpu_radix_join execution method
+  (radix-join/src/execution_methods/gpu_radix_join.rs:90-565);
+* the seeded generator (``gen_*``).
+
+Every call goes through the compiled library ``libfi_sqlops.so`` next to this
+file; there is no other code path.  Errors raise ``SqlOpsError`` whose ``kind``
+names the reference's ErrorKind (sql-ops/src/error.rs:20-29).
+"""
+import ctypes as C
+import enum
+import os
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfi_sqlops.so")
+
+PADDING_BYTES = 128
+ALIGN_BYTES = 128
+RADIX_JOIN_BUCKET_CHAINING_ENTRIES = 2048
+
+_ERR_KIND = {
+    -1: "InvalidArgument",
+    -2: "IntegerOverflow",
+    -3: "CudaError",
+    -4: "RuntimeError",
+    -5: "Timeout",
+    -6: "Unsupported",
+    -7: "Capacity",
+    -8: "OutOfMemory",
+}
+
+
+class SqlOpsError(RuntimeError):
+    def __init__(self, code, message):
+        self.code = code
+        self.kind = _ERR_KIND.get(code, "Unknown")
+        super().__init__("%s: %s" % (self.kind, message))
+
+
+_lib = None
+
+
+def lib():
+    """The compiled library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(
+                "libfi_sqlops.so is missing; build it with "
+                "`make -C fast-interconnects_b200` (or __graft_entry__.build())")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.fi_last_error.restype = C.c_char_p
+        _lib.fi_version.restype = C.c_char_p
+        _lib.fi_padding_len.restype = C.c_uint32
+        _lib.fi_partitioned_relation_alloc_len.restype = C.c_uint64
+        _lib.fi_radix_join_engine_workspace_bytes.restype = C.c_uint64
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise SqlOpsError(rc, lib().fi_last_error().decode())
+
+
+# ---------------------------------------------------------------------------
+# vocabulary
+# ---------------------------------------------------------------------------
+class GpuHistogramAlgorithm(enum.IntEnum):
+    Chunked = 0
+    Contiguous = 1
+
+
+HistogramAlgorithmType = GpuHistogramAlgorithm
+
+
+class GpuRadixPartitionAlgorithm(enum.IntEnum):
+    NC = 0
+    LASWWC = 1
+    SSWWCv2 = 2
+    SSWWCv2G = 3
+    HSSWWCv4 = 4
+
+
+class RadixPass(enum.IntEnum):
+    First = 0
+    Second = 1
+    Third = 2
+
+
+class HashingScheme(enum.IntEnum):
+    Perfect = 0
+    LinearProbing = 1
+    BucketChaining = 2
+
+
+class _RadixBitsC(C.Structure):
+    _fields_ = [("pass_bits", C.c_int32 * 3)]
+
+
+class RadixBits:
+    """RadixBits (partition.rs:64-110)."""
+
+    def __init__(self, first=None, second=None, third=None):
+        self.pass_bits = [first, second, third]
+
+    def c(self):
+        return _RadixBitsC((C.c_int32 * 3)(
+            *[-1 if b is None else b for b in self.pass_bits]))
+
+    def pass_radix_bits(self, p):
+        return self.pass_bits[int(p)]
+
+    def pass_fanout(self, p):
+        b = self.pass_bits[int(p)]
+        return None if b is None else 1 << b
+
+    def pass_ignore_bits(self, p):
+        return sum(b or 0 for b in self.pass_bits[:int(p)])
+
+    def radix_bits(self):
+        return sum(b or 0 for b in self.pass_bits)
+
+
+class _OffsetsC(C.Structure):
+    _fields_ = [("offsets", C.c_void_p), ("local_offsets", C.c_void_p),
+                ("chunks", C.c_uint32), ("max_chunks", C.c_uint32),
+                ("radix_bits", C.c_uint32), ("histogram_type", C.c_uint32),
+                ("data_len", C.c_uint64), ("has_data_len", C.c_uint32),
+                ("tuple_bytes", C.c_uint32)]
+
+
+class _RelationC(C.Structure):
+    _fields_ = [("relation", C.c_void_p), ("relation_len", C.c_uint64),
+                ("offsets", C.c_void_p), ("len", C.c_uint64),
+                ("chunks", C.c_uint32), ("radix_bits", C.c_uint32),
+                ("tuple_bytes", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _JoinResultC(C.Structure):
+    _fields_ = [("sum", C.c_int64), ("count", C.c_uint64)]
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _tuple_bytes(dtype):
+    return 8 if dtype == torch.int32 else 16
+
+
+def _sfx(dtype):
+    if dtype == torch.int32:
+        return "int32"
+    if dtype == torch.int64:
+        return "int64"
+    raise TypeError("keys must be int32 or int64 (gpu_radix_partition.rs:1245)")
+
+
+def padding_len(dtype):
+    return lib().fi_padding_len(_tuple_bytes(dtype))
+
+
+def input_chunk_size(data_len, num_chunks, key_bytes):
+    out = C.c_uint64(0)
+    _check(lib().fi_input_chunk_size(C.c_uint64(data_len), C.c_uint32(num_chunks),
+                                     C.c_uint32(key_bytes), C.byref(out)))
+    return out.value
+
+
+# ---------------------------------------------------------------------------
+# PartitionOffsets / PartitionedRelation
+# ---------------------------------------------------------------------------
+class PartitionOffsets:
+    """PartitionOffsets<Tuple<K,K>> (partitioned_relation.rs:62-201).
+
+    Memory: u64 tensors on `device` (pass 'cpu' with pin=True for pinned host
+    memory the GPU can address, like the reference's CudaPinnedMem)."""
+
+    def __init__(self, histogram_type, max_chunks, radix_bits, dtype,
+                 device="cuda", pin=False):
+        F = 1 << radix_bits
+        chunks = max_chunks if histogram_type == GpuHistogramAlgorithm.Chunked else 1
+        self.dtype = dtype
+        self.offsets = _alloc_u64(chunks * F, device, pin)
+        self.local_offsets = (_alloc_u64(max_chunks * F, device, pin)
+                              if histogram_type == GpuHistogramAlgorithm.Contiguous
+                              else None)
+        self.c = _OffsetsC()
+        _check(lib().fi_partition_offsets_init(
+            C.byref(self.c), C.c_int(int(histogram_type)), C.c_uint32(max_chunks),
+            C.c_uint32(radix_bits), C.c_uint32(_tuple_bytes(dtype)),
+            _ptr(self.offsets), _ptr(self.local_offsets)))
+
+    def _sync_ptrs(self):
+        self.c.offsets = self.offsets.data_ptr()
+
+    def num_chunks(self):
+        return self.c.chunks
+
+    def radix_bits(self):
+        return self.c.radix_bits
+
+    def fanout(self):
+        return 1 << self.c.radix_bits
+
+    def len(self):
+        return self.c.data_len if self.c.has_data_len else None
+
+    def padding_len(self):
+        return padding_len(self.dtype)
+
+
+def _alloc_u64(n, device, pin):
+    t = torch.empty(max(n, 1), dtype=torch.int64,
+                    device=device if not pin else "cpu",
+                    pin_memory=pin)
+    return t
+
+
+class PartitionedRelation:
+    """PartitionedRelation<Tuple<K,K>> (partitioned_relation.rs:323-497).
+    `relation` is an (alloc_len, 2) tensor; `offsets` a u64 tensor."""
+
+    def __init__(self, length, histogram_type, radix_bits, max_chunks, dtype,
+                 device="cuda", fill=None):
+        alloc = lib().fi_partitioned_relation_alloc_len(
+            C.c_uint64(length), C.c_int(int(histogram_type)),
+            C.c_uint32(radix_bits), C.c_uint32(max_chunks),
+            C.c_uint32(_tuple_bytes(dtype)))
+        self.dtype = dtype
+        if fill is None:
+            self.relation = torch.empty((max(alloc, 1), 2), dtype=dtype, device=device)
+        else:
+            self.relation = torch.full((max(alloc, 1), 2), fill, dtype=dtype,
+                                       device=device)
+        chunks = max_chunks if histogram_type == GpuHistogramAlgorithm.Chunked else 1
+        self.offsets = torch.zeros(chunks << radix_bits, dtype=torch.int64,
+                                   device=device)
+        self.c = _RelationC()
+        _check(lib().fi_partitioned_relation_init(
+            C.byref(self.c), C.c_uint64(length), C.c_int(int(histogram_type)),
+            C.c_uint32(radix_bits), C.c_uint32(max_chunks),
+            C.c_uint32(_tuple_bytes(dtype)), _ptr(self.relation),
+            C.c_uint64(alloc), _ptr(self.offsets)))
+
+    def _sync_ptrs(self):
+        self.c.offsets = self.offsets.data_ptr()
+
+    def len(self):
+        return self.c.len
+
+    def num_chunks(self):
+        return self.c.chunks
+
+    def radix_bits(self):
+        return self.c.radix_bits
+
+    def fanout(self):
+        return 1 << self.c.radix_bits
+
+    def padding_len(self):
+        return padding_len(self.dtype)
+
+    def padded_len(self):
+        return self.c.len + (self.c.chunks << self.c.radix_bits) * self.padding_len()
+
+    def resize(self, new_len):
+        _check(lib().fi_partitioned_relation_resize(C.byref(self.c),
+                                                    C.c_uint64(new_len)))
+
+    def partition_len(self, partition_id):
+        host = self.offsets.cpu().contiguous()
+        out = C.c_uint64(0)
+        _check(lib().fi_partition_len(C.byref(self.c), _ptr(host),
+                                      C.c_uint32(partition_id), C.byref(out)))
+        return out.value
+
+
+# ---------------------------------------------------------------------------
+# GpuRadixPartitioner
+# ---------------------------------------------------------------------------
+class GpuRadixPartitioner:
+    """GpuRadixPartitioner (gpu_radix_partition.rs:314-555)."""
+
+    def __init__(self, prefix_sum_algorithm, partition_algorithm, radix_bits,
+                 grid_size, block_size, dmem_buffer_bytes=8192):
+        self.h = C.c_void_p()
+        self.radix_bits = radix_bits
+        _check(lib().fi_gpu_radix_partitioner_new(
+            C.c_int(int(prefix_sum_algorithm)), C.c_int(int(partition_algorithm)),
+            radix_bits.c(), C.c_uint32(grid_size), C.c_uint32(block_size),
+            C.c_uint64(dmem_buffer_bytes), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fi_gpu_radix_partitioner_free(self.h)
+            self.h = None
+
+    def status(self):
+        _check(lib().fi_gpu_radix_partitioner_status(self.h))
+
+    def prefix_sum(self, radix_pass, partition_attr, partition_offsets,
+                   stream=None):
+        f = getattr(lib(), "fi_gpu_prefix_sum_" + _sfx(partition_attr.dtype))
+        _check(f(self.h, C.c_int(int(radix_pass)), _ptr(partition_attr),
+                 C.c_uint64(partition_attr.numel()),
+                 C.byref(partition_offsets.c), _stream(stream)))
+
+    def prefix_sum_and_copy_with_payload(self, radix_pass, src_key, src_pay,
+                                         dst_key, dst_pay, partition_offsets,
+                                         stream=None):
+        f = getattr(lib(), "fi_gpu_prefix_sum_and_copy_with_payload_" +
+                    _sfx(src_key.dtype))
+        _check(f(self.h, C.c_int(int(radix_pass)), _ptr(src_key), _ptr(src_pay),
+                 C.c_uint64(src_key.numel()), _ptr(dst_key), _ptr(dst_pay),
+                 C.c_uint64(dst_key.numel()), C.byref(partition_offsets.c),
+                 _stream(stream)))
+
+    def prefix_sum_and_transform(self, radix_pass, partition_id, src_relation,
+                                 dst_key, dst_pay, partition_offsets,
+                                 stream=None):
+        f = getattr(lib(), "fi_gpu_prefix_sum_and_transform_" + _sfx(dst_key.dtype))
+        _check(f(self.h, C.c_int(int(radix_pass)), C.c_uint32(partition_id),
+                 C.byref(src_relation.c), _ptr(dst_key), _ptr(dst_pay),
+                 C.c_uint64(dst_key.numel()), C.byref(partition_offsets.c),
+                 _stream(stream)))
+
+    def preallocate_partition_state(self, radix_pass, dtype=torch.int64):
+        f = getattr(lib(), "fi_gpu_preallocate_partition_state_" + _sfx(dtype))
+        _check(f(self.h, C.c_int(int(radix_pass))))
+
+    def partition(self, radix_pass, partition_attr, payload_attr,
+                  partition_offsets, partitioned_relation, stream=None):
+        """Partitions and swaps the offsets into the relation
+        (gpu_radix_partition.rs:1113-1121)."""
+        if partition_attr.numel() != payload_attr.numel():
+            raise SqlOpsError(-1, "Partition and payload attributes have "
+                                  "different sizes")
+        f = getattr(lib(), "fi_gpu_partition_" + _sfx(partition_attr.dtype))
+        before = partition_offsets.c.offsets
+        _check(f(self.h, C.c_int(int(radix_pass)), _ptr(partition_attr),
+                 _ptr(payload_attr), C.c_uint64(partition_attr.numel()),
+                 C.byref(partition_offsets.c), C.byref(partitioned_relation.c),
+                 _stream(stream)))
+        if partitioned_relation.c.offsets == before:
+            partition_offsets.offsets, partitioned_relation.offsets = (
+                partitioned_relation.offsets, partition_offsets.offsets)
+
+
+# ---------------------------------------------------------------------------
+# CudaRadixJoin
+# ---------------------------------------------------------------------------
+class CudaRadixJoin:
+    """CudaRadixJoin (cuda_radix_join.rs:116-164)."""
+
+    def __init__(self, radix_pass, radix_bits, hashing_scheme, grid_size,
+                 block_size):
+        self.h = C.c_void_p()
+        self.grid_size, self.block_size = grid_size, block_size
+        _check(lib().fi_cuda_radix_join_new(
+            C.c_int(int(radix_pass)), radix_bits.c(), C.c_int(int(hashing_scheme)),
+            C.c_uint32(grid_size), C.c_uint32(block_size), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fi_cuda_radix_join_free(self.h)
+            self.h = None
+
+    def status(self):
+        _check(lib().fi_cuda_radix_join_status(self.h))
+
+    def join(self, build_rel, probe_rel, result_set, task_assignments,
+             match_count=None, stream=None):
+        f = getattr(lib(), "fi_cuda_radix_join_" + _sfx(build_rel.dtype))
+        _check(f(self.h, C.byref(build_rel.c), C.byref(probe_rel.c),
+                 _ptr(result_set), C.c_uint64(result_set.numel()),
+                 _ptr(task_assignments), C.c_uint64(task_assignments.numel()),
+                 _ptr(match_count), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# CudaHashJoin (no partitioning)
+# ---------------------------------------------------------------------------
+class HashTable:
+    """HashTable::new_on_gpu (no_partitioning_join.rs:579-625)."""
+
+    def __init__(self, size, dtype, mem_len=None, stream=None):
+        mem_len = size if mem_len is None else mem_len
+        self.dtype = dtype
+        self.size = size
+        self.mem = torch.empty((max(mem_len, 1), 2), dtype=dtype, device="cuda")
+        f = getattr(lib(), "fi_hash_table_init_" + _sfx(dtype))
+        _check(f(_ptr(self.mem), C.c_uint64(mem_len), _stream(stream)))
+
+
+class CudaHashJoin:
+    """CudaHashJoin built like CudaHashJoinBuilder (no_partitioning_join.rs)."""
+
+    def __init__(self, hashing_scheme, hash_table, build_dim=(1, 1),
+                 probe_dim=(1, 1), is_selective=False):
+        self.ht = hash_table
+        self.h = C.c_void_p()
+        _check(lib().fi_cuda_hash_join_new(
+            C.c_int(int(hashing_scheme)), C.c_int(1 if is_selective else 0),
+            _ptr(hash_table.mem), C.c_uint64(hash_table.mem.shape[0]),
+            C.c_uint64(hash_table.size), C.c_uint32(build_dim[0]),
+            C.c_uint32(build_dim[1]), C.c_uint32(probe_dim[0]),
+            C.c_uint32(probe_dim[1]), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fi_cuda_hash_join_free(self.h)
+            self.h = None
+
+    def build(self, join_attr, payload_attr, stream=None):
+        f = getattr(lib(), "fi_cuda_hash_join_build_" + _sfx(join_attr.dtype))
+        _check(f(self.h, _ptr(join_attr), _ptr(payload_attr),
+                 C.c_uint64(join_attr.numel()), _stream(stream)))
+
+    def probe_sum(self, join_attr, payload_attr, result_set, stream=None):
+        f = getattr(lib(), "fi_cuda_hash_join_probe_sum_" + _sfx(join_attr.dtype))
+        _check(f(self.h, _ptr(join_attr), _ptr(payload_attr),
+                 C.c_uint64(join_attr.numel()), _ptr(result_set),
+                 C.c_uint64(result_set.numel()), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# gpu_radix_join execution method
+# ---------------------------------------------------------------------------
+class RadixJoinEngine:
+    """Whole radix join (pass 1, optional pass 2, per-partition join)."""
+
+    def __init__(self, max_build, max_probe, dtype, radix_bits,
+                 hashing_scheme=HashingScheme.BucketChaining):
+        self.dtype = dtype
+        self.h = C.c_void_p()
+        _check(lib().fi_radix_join_engine_new(
+            C.c_uint64(max_build), C.c_uint64(max_probe),
+            C.c_uint32(_tuple_bytes(dtype)), radix_bits.c(),
+            C.c_int(int(hashing_scheme)), C.byref(self.h)))
+        self.result = torch.zeros(2, dtype=torch.int64, device="cuda")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fi_radix_join_engine_free(self.h)
+            self.h = None
+
+    def workspace_bytes(self):
+        return lib().fi_radix_join_engine_workspace_bytes(self.h)
+
+    PHASE_EVENTS = 11
+
+    def set_events(self, events):
+        """Records torch.cuda.Event objects at the phase boundaries of every
+        run (see fi_radix_join_engine_set_events); None stops recording."""
+        if events is None:
+            _check(lib().fi_radix_join_engine_set_events(self.h, None, 0))
+            self._events = None
+            return
+        arr = (C.c_void_p * len(events))(*[e.cuda_event for e in events])
+        self._events = (events, arr)
+        _check(lib().fi_radix_join_engine_set_events(self.h, arr, len(events)))
+
+    def last_launches(self):
+        return lib().fi_radix_join_engine_last_launches(self.h)
+
+    def status(self):
+        _check(lib().fi_radix_join_engine_status(self.h))
+
+    def run_async(self, build_key, build_pay, probe_key, probe_pay, stream=None):
+        """Enqueues the join; the device tensor self.result = [sum, count]."""
+        f = getattr(lib(), "fi_radix_join_engine_run_" + _sfx(build_key.dtype))
+        _check(f(self.h, _ptr(build_key), _ptr(build_pay),
+                 C.c_uint64(build_key.numel()), _ptr(probe_key), _ptr(probe_pay),
+                 C.c_uint64(probe_key.numel()), _ptr(self.result), _stream(stream)))
+        return self.result
+
+    def run(self, build_key, build_pay, probe_key, probe_pay, stream=None):
+        self.run_async(build_key, build_pay, probe_key, probe_pay, stream)
+        r = self.result.cpu()
+        return int(r[0]), int(r[1]) & ((1 << 64) - 1)
+
+    def run_host(self, build_key, build_pay, probe_key, probe_pay, stream=None):
+        """Host (pinned) int64 columns in, (sum, count) out; synchronous."""
+        res = _JoinResultC()
+        _check(lib().fi_radix_join_engine_run_host_int64(
+            self.h, _ptr(build_key), _ptr(build_pay),
+            C.c_uint64(build_key.numel()), _ptr(probe_key), _ptr(probe_pay),
+            C.c_uint64(probe_key.numel()), C.byref(res), _stream(stream)))
+        return res.sum, res.count
+
+
+# ---------------------------------------------------------------------------
+# seeded generator
+# ---------------------------------------------------------------------------
+def _ctype(dtype):
+    return C.c_int32 if dtype == torch.int32 else C.c_int64
+
+
+def gen_primary_keys(t, seed, base=1, stream=None):
+    f = getattr(lib(), "fi_datagen_primary_keys_" + _sfx(t.dtype))
+    _check(f(_ptr(t), C.c_uint64(t.numel()), C.c_uint64(seed),
+             _ctype(t.dtype)(base), _stream(stream)))
+    return t
+
+
+def gen_uniform_foreign_keys(t, pk_n, seed, base=1, stream=None):
+    f = getattr(lib(), "fi_datagen_uniform_foreign_keys_" + _sfx(t.dtype))
+    _check(f(_ptr(t), C.c_uint64(t.numel()), C.c_uint64(pk_n), C.c_uint64(seed),
+             _ctype(t.dtype)(base), _stream(stream)))
+    return t
+
+
+def gen_zipf_foreign_keys(t, pk_n, s, seed, pk_seed, base=1, stream=None):
+    f = getattr(lib(), "fi_datagen_zipf_foreign_keys_" + _sfx(t.dtype))
+    _check(f(_ptr(t), C.c_uint64(t.numel()), C.c_uint64(pk_n), C.c_double(s),
+             C.c_uint64(seed), C.c_uint64(pk_seed), _ctype(t.dtype)(base),
+             _stream(stream)))
+    return t
+
+
+def gen_uniform_u64_keys(t, seed, stream=None):
+    _check(lib().fi_datagen_uniform_u64_keys(_ptr(t), C.c_uint64(t.numel()),
+                                             C.c_uint64(seed), _stream(stream)))
+    return t

@@ -1,0 +1,425 @@
+/*
+ * fi_sqlops.h -- C ABI of the B200 (sm_100a) radix-partition and hash-join
+ * operators.
+ *
+ * This is the drop-in boundary for the reference's `sql-ops` crate: every
+ * entry point below replaces the body of one Rust API call of the reference
+ * (cited per declaration, paths relative to the reference project root) and
+ * keeps that call's argument meaning, memory layout and error behaviour.  A
+ * Rust binding is a plain `extern "C"` block over these declarations.
+ *
+ * Conventions
+ *  - Every function returns `int` status: FI_OK (0) or a negative FI_ERR_*
+ *    code (the reference's ErrorKind, sql-ops/src/error.rs:20-29).  No entry
+ *    point aborts the process; fi_last_error() returns a thread-local message.
+ *  - Pointers are device pointers (or any memory the GPU can address, such as
+ *    pinned or managed memory) unless a parameter says "host".
+ *  - Work is enqueued on the caller's CUDA stream (`cudaStream_t` passed as
+ *    fi_stream_t); functions return before the GPU has finished, exactly as
+ *    the reference's launches do.  A CUDA context must be current.
+ *  - Handles are not thread-safe for concurrent callers (like
+ *    GpuRadixPartitioner, gpu_radix_partition.rs:396-399).
+ *  - Tuples are `{K key; K value;}` with K = int32_t or int64_t
+ *    (Tuple<K,V>, sql-ops/src/partition.rs:144-147); padding in front of
+ *    every partition is PADDING_BYTES = 128 bytes (sql-ops/build.rs:58).
+ *  - Device-side waits are bounded.  A wait that gives up records
+ *    FI_ERR_TIMEOUT in the handle; fi_*_status() reports it.
+ */
+#ifndef FI_SQLOPS_H
+#define FI_SQLOPS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without including the CUDA headers. */
+typedef struct CUstream_st *fi_stream_t;
+
+/* ---- status codes: sql-ops/src/error.rs:20-29 ------------------------- */
+#define FI_OK 0
+#define FI_ERR_INVALID_ARGUMENT (-1) /* ErrorKind::InvalidArgument */
+#define FI_ERR_INTEGER_OVERFLOW (-2) /* ErrorKind::IntegerOverflow */
+#define FI_ERR_CUDA (-3)             /* ErrorKind::CudaError */
+#define FI_ERR_RUNTIME (-4)          /* ErrorKind::RuntimeError */
+#define FI_ERR_TIMEOUT (-5)          /* a bounded device wait gave up */
+#define FI_ERR_UNSUPPORTED (-6)      /* `unimplemented!()` in the reference */
+#define FI_ERR_CAPACITY (-7)         /* hash-table / shared-memory capacity */
+#define FI_ERR_OUT_OF_MEMORY (-8)    /* device allocation failed */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *fi_last_error(void);
+
+/* Version string of the library. */
+const char *fi_version(void);
+
+/* ---- vocabulary: sql-ops/src/partition.rs:35-134 ----------------------- */
+/* HistogramAlgorithmType / GpuHistogramAlgorithm
+ * (partition.rs:35-46, gpu_radix_partition.rs:192-222) */
+typedef enum {
+  FI_HISTOGRAM_CHUNKED = 0,
+  FI_HISTOGRAM_CONTIGUOUS = 1
+} fi_histogram_algorithm;
+
+/* GpuRadixPartitionAlgorithm (gpu_radix_partition.rs:233-293).  All five
+ * produce the same partitions; on B200 they select between the per-tuple
+ * scatter (NC) and the shared-memory tile write-combining scatter (the
+ * others), and HSSWWC_V4 also selects the hierarchical two-level scatter for
+ * fanouts above 2^11. */
+typedef enum {
+  FI_PARTITION_NC = 0,
+  FI_PARTITION_LASWWC = 1,
+  FI_PARTITION_SSWWC_V2 = 2,
+  FI_PARTITION_SSWWC_V2G = 3,
+  FI_PARTITION_HSSWWC_V4 = 4
+} fi_partition_algorithm;
+
+/* RadixPass (partition.rs:56-60) */
+typedef enum { FI_PASS_FIRST = 0, FI_PASS_SECOND = 1, FI_PASS_THIRD = 2 } fi_radix_pass;
+
+/* HashingScheme (sql-ops/src/join/hashing_scheme.rs:18-43) */
+typedef enum {
+  FI_HASHING_PERFECT = 0,
+  FI_HASHING_LINEAR_PROBING = 1,
+  FI_HASHING_BUCKET_CHAINING = 2
+} fi_hashing_scheme;
+
+/* RadixBits (partition.rs:64-110): bits per pass; a negative value means the
+ * pass is absent (`None`). */
+typedef struct {
+  int32_t pass_bits[3];
+} fi_radix_bits;
+
+/* PartitionOffsets<Tuple<K,K>> (partitioned_relation.rs:62-201).
+ * Chunk-major `offsets` (C0.P0 .. C0.PF-1, C1.P0, ...): chunks = max_chunks
+ * for Chunked, 1 for Contiguous.  `local_offsets` ([max_chunks * fanout],
+ * Contiguous only, NULL otherwise) is the per-chunk cursor array that the
+ * Contiguous prefix sum hands to `partition`.  `data_len` is set by the
+ * prefix-sum calls.  Memory is owned by the caller. */
+typedef struct {
+  uint64_t *offsets;
+  uint64_t *local_offsets;
+  uint32_t chunks;
+  uint32_t max_chunks;
+  uint32_t radix_bits;
+  uint32_t histogram_type; /* fi_histogram_algorithm */
+  uint64_t data_len;
+  uint32_t has_data_len;
+  uint32_t tuple_bytes; /* 8 (int32 tuples) or 16 (int64 tuples) */
+} fi_partition_offsets;
+
+/* PartitionedRelation<Tuple<K,K>> (partitioned_relation.rs:323-497).
+ * `relation` holds len + chunks*fanout*padding tuples (relation_len is the
+ * allocated number of tuples, >= that); partition (c,p) spans
+ * [offsets[c*F+p], offsets[c*F+p+1] - padding), the last one ends at
+ * len + chunks*fanout*padding (index rule :510-537).  Memory is owned by the
+ * caller; `partition` swaps the offsets pointer with the PartitionOffsets'
+ * one (gpu_radix_partition.rs:1117-1121). */
+typedef struct {
+  void *relation;
+  uint64_t relation_len;
+  uint64_t *offsets;
+  uint64_t len;
+  uint32_t chunks;
+  uint32_t radix_bits;
+  uint32_t tuple_bytes;
+  uint32_t reserved;
+} fi_partitioned_relation;
+
+/* ---- host-side helpers (no GPU needed) --------------------------------- */
+
+/* input_chunk_size (sql-ops/src/partition/partition_input_chunk.rs:24-35):
+ * ceil(len/chunks) rounded down to ALIGN_BYTES/key_bytes.  Returns
+ * FI_ERR_INTEGER_OVERFLOW when the chunk length is >= 2^32-1. */
+int fi_input_chunk_size(uint64_t data_len, uint32_t num_chunks,
+                        uint32_t key_bytes, uint64_t *chunk_len);
+
+/* Number of padding tuples per partition: PADDING_BYTES / tuple_bytes
+ * (partitioned_relation.rs:27-29). */
+uint32_t fi_padding_len(uint32_t tuple_bytes);
+
+/* PartitionOffsets::new (partitioned_relation.rs:74-103) on caller memory:
+ * fills the descriptor; `offsets` must hold chunks*fanout entries and, for
+ * Contiguous, `local_offsets` max_chunks*fanout entries. */
+int fi_partition_offsets_init(fi_partition_offsets *o,
+                              fi_histogram_algorithm histogram_type,
+                              uint32_t max_chunks, uint32_t radix_bits,
+                              uint32_t tuple_bytes, uint64_t *offsets,
+                              uint64_t *local_offsets);
+
+/* PartitionedRelation::new (partitioned_relation.rs:335-362) on caller
+ * memory; `relation` must hold fi_partitioned_relation_alloc_len() tuples. */
+int fi_partitioned_relation_init(fi_partitioned_relation *r, uint64_t len,
+                                 fi_histogram_algorithm histogram_type,
+                                 uint32_t radix_bits, uint32_t max_chunks,
+                                 uint32_t tuple_bytes, void *relation,
+                                 uint64_t relation_len, uint64_t *offsets);
+
+/* len + chunks*fanout*padding: tuples to allocate for a PartitionedRelation
+ * (partitioned_relation.rs:347-352). */
+uint64_t fi_partitioned_relation_alloc_len(uint64_t len,
+                                           fi_histogram_algorithm histogram_type,
+                                           uint32_t radix_bits,
+                                           uint32_t max_chunks,
+                                           uint32_t tuple_bytes);
+
+/* PartitionedRelation::partition_len (partitioned_relation.rs:409-437);
+ * `host_offsets` are the relation's offsets as host-readable memory. */
+int fi_partition_len(const fi_partitioned_relation *r,
+                     const uint64_t *host_offsets, uint32_t partition_id,
+                     uint64_t *len);
+
+/* PartitionedRelation::resize (partitioned_relation.rs:383-395). */
+int fi_partitioned_relation_resize(fi_partitioned_relation *r,
+                                   uint64_t new_len);
+
+/* ---- GpuRadixPartitioner (gpu_radix_partition.rs:314-555) -------------- */
+typedef struct fi_gpu_radix_partitioner fi_gpu_radix_partitioner;
+
+/* GpuRadixPartitioner::new (gpu_radix_partition.rs:329-383).  grid_size is
+ * the number of chunks of the Chunked layout; block_size and
+ * dmem_buffer_bytes are tuning hints. */
+int fi_gpu_radix_partitioner_new(fi_histogram_algorithm prefix_sum_algorithm,
+                                 fi_partition_algorithm partition_algorithm,
+                                 fi_radix_bits radix_bits, uint32_t grid_size,
+                                 uint32_t block_size,
+                                 uint64_t dmem_buffer_bytes,
+                                 fi_gpu_radix_partitioner **out);
+void fi_gpu_radix_partitioner_free(fi_gpu_radix_partitioner *p);
+
+/* Synchronises the device and reports (and clears) a device-side error the
+ * partitioner's kernels recorded (FI_ERR_TIMEOUT, FI_ERR_CAPACITY). */
+int fi_gpu_radix_partitioner_status(fi_gpu_radix_partitioner *p);
+
+/* GpuRadixPartitioner::prefix_sum (gpu_radix_partition.rs:400-408, impl
+ * :561-696): histogram + exclusive prefix sum + padding -> offsets (Chunked)
+ * or offsets + local_offsets (Contiguous). */
+int fi_gpu_prefix_sum_int32(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
+                            const int32_t *partition_attr, uint64_t len,
+                            fi_partition_offsets *offsets, fi_stream_t stream);
+int fi_gpu_prefix_sum_int64(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
+                            const int64_t *partition_attr, uint64_t len,
+                            fi_partition_offsets *offsets, fi_stream_t stream);
+
+/* GpuRadixPartitioner::prefix_sum_and_copy_with_payload
+ * (gpu_radix_partition.rs:431-451, impl :698-824): Contiguous prefix sum
+ * that also copies both columns to dst (dst_len must equal len). */
+int fi_gpu_prefix_sum_and_copy_with_payload_int32(
+    fi_gpu_radix_partitioner *p, fi_radix_pass pass, const int32_t *src_key,
+    const int32_t *src_pay, uint64_t len, int32_t *dst_key, int32_t *dst_pay,
+    uint64_t dst_len, fi_partition_offsets *offsets, fi_stream_t stream);
+int fi_gpu_prefix_sum_and_copy_with_payload_int64(
+    fi_gpu_radix_partitioner *p, fi_radix_pass pass, const int64_t *src_key,
+    const int64_t *src_pay, uint64_t len, int64_t *dst_key, int64_t *dst_pay,
+    uint64_t dst_len, fi_partition_offsets *offsets, fi_stream_t stream);
+
+/* GpuRadixPartitioner::prefix_sum_and_transform
+ * (gpu_radix_partition.rs:480-500, impl :826-957): gathers partition
+ * `partition_id` of every chunk of `src` (whose offsets must be device
+ * readable) into the columns dst_key/dst_pay (dst_len = that partition's
+ * length) and computes their Contiguous prefix sum. */
+int fi_gpu_prefix_sum_and_transform_int32(
+    fi_gpu_radix_partitioner *p, fi_radix_pass pass, uint32_t partition_id,
+    const fi_partitioned_relation *src, int32_t *dst_key, int32_t *dst_pay,
+    uint64_t dst_len, fi_partition_offsets *offsets, fi_stream_t stream);
+int fi_gpu_prefix_sum_and_transform_int64(
+    fi_gpu_radix_partitioner *p, fi_radix_pass pass, uint32_t partition_id,
+    const fi_partitioned_relation *src, int64_t *dst_key, int64_t *dst_pay,
+    uint64_t dst_len, fi_partition_offsets *offsets, fi_stream_t stream);
+
+/* GpuRadixPartitioner::preallocate_partition_state
+ * (gpu_radix_partition.rs:511-526): allocates the internal device state of
+ * `partition` ahead of time. */
+int fi_gpu_preallocate_partition_state_int32(fi_gpu_radix_partitioner *p,
+                                             fi_radix_pass pass);
+int fi_gpu_preallocate_partition_state_int64(fi_gpu_radix_partitioner *p,
+                                             fi_radix_pass pass);
+
+/* GpuRadixPartitioner::partition (gpu_radix_partition.rs:536-554, impl
+ * :1022-1239): scatters (key, payload) into `rel`; swaps the offsets into
+ * the relation (the PartitionOffsets becomes "uninitialised but reusable"). */
+int fi_gpu_partition_int32(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
+                           const int32_t *partition_attr,
+                           const int32_t *payload_attr, uint64_t len,
+                           fi_partition_offsets *offsets,
+                           fi_partitioned_relation *rel, fi_stream_t stream);
+int fi_gpu_partition_int64(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
+                           const int64_t *partition_attr,
+                           const int64_t *payload_attr, uint64_t len,
+                           fi_partition_offsets *offsets,
+                           fi_partitioned_relation *rel, fi_stream_t stream);
+
+/* ---- CudaRadixJoin (sql-ops/src/join/cuda_radix_join.rs:116-164) ------ */
+typedef struct fi_cuda_radix_join fi_cuda_radix_join;
+
+/* CudaRadixJoin::new (cuda_radix_join.rs:127-142). */
+int fi_cuda_radix_join_new(fi_radix_pass radix_pass, fi_radix_bits radix_bits,
+                           fi_hashing_scheme hashing_scheme, uint32_t grid_size,
+                           uint32_t block_size, fi_cuda_radix_join **out);
+void fi_cuda_radix_join_free(fi_cuda_radix_join *j);
+int fi_cuda_radix_join_status(fi_cuda_radix_join *j);
+
+/* CudaRadixJoin::join (cuda_radix_join.rs:144-163, impl :172-276):
+ * SELECT SUM(s.value) FROM build r JOIN probe s ON r.key = s.key, per
+ * partition of two Contiguous relations.  result_set[grid*block] receives
+ * per-thread i64 sums with `+=` (the caller zeroes it); task_assignments
+ * ([grid+1]) receives the reference's greedy partition ranges
+ * (radix_join.cu:58-98).  match_count (optional, may be NULL) is a device
+ * u64 that receives `+=` the number of matches. */
+int fi_cuda_radix_join_int32(fi_cuda_radix_join *j,
+                             const fi_partitioned_relation *build_rel,
+                             const fi_partitioned_relation *probe_rel,
+                             int64_t *result_set, uint64_t result_len,
+                             uint32_t *task_assignments, uint64_t task_len,
+                             uint64_t *match_count, fi_stream_t stream);
+int fi_cuda_radix_join_int64(fi_cuda_radix_join *j,
+                             const fi_partitioned_relation *build_rel,
+                             const fi_partitioned_relation *probe_rel,
+                             int64_t *result_set, uint64_t result_len,
+                             uint32_t *task_assignments, uint64_t task_len,
+                             uint64_t *match_count, fi_stream_t stream);
+
+/* ---- CudaHashJoin: no-partitioning join
+ *      (sql-ops/src/join/no_partitioning_join.rs:153-304) -------------- */
+typedef struct fi_cuda_hash_join fi_cuda_hash_join;
+
+/* HashTable::new_on_gpu (no_partitioning_join.rs:579-625): sets every key of
+ * `mem_len` entries to the null key. */
+int fi_hash_table_init_int32(void *ht_mem, uint64_t mem_len, fi_stream_t stream);
+int fi_hash_table_init_int64(void *ht_mem, uint64_t mem_len, fi_stream_t stream);
+
+/* CudaHashJoinBuilder::build (no_partitioning_join.rs:688-735).  ht_mem holds
+ * ht_mem_len entries; ht_size is the table size used for hashing. */
+int fi_cuda_hash_join_new(fi_hashing_scheme hashing_scheme, int is_selective,
+                          void *ht_mem, uint64_t ht_mem_len, uint64_t ht_size,
+                          uint32_t build_grid, uint32_t build_block,
+                          uint32_t probe_grid, uint32_t probe_block,
+                          fi_cuda_hash_join **out);
+void fi_cuda_hash_join_free(fi_cuda_hash_join *hj);
+
+/* CudaHashJoin::build (no_partitioning_join.rs:250-258, impl :333-386). */
+int fi_cuda_hash_join_build_int32(fi_cuda_hash_join *hj, const int32_t *key,
+                                  const int32_t *pay, uint64_t len,
+                                  fi_stream_t stream);
+int fi_cuda_hash_join_build_int64(fi_cuda_hash_join *hj, const int64_t *key,
+                                  const int64_t *pay, uint64_t len,
+                                  fi_stream_t stream);
+
+/* CudaHashJoin::probe_sum (no_partitioning_join.rs:266-279, impl :388-433):
+ * result_set[probe_grid*probe_block] receives per-thread u64 sums (`+=`). */
+int fi_cuda_hash_join_probe_sum_int32(fi_cuda_hash_join *hj,
+                                      const int32_t *key, const int32_t *pay,
+                                      uint64_t len, uint64_t *result_set,
+                                      uint64_t result_len, fi_stream_t stream);
+int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
+                                      const int64_t *key, const int64_t *pay,
+                                      uint64_t len, uint64_t *result_set,
+                                      uint64_t result_len, fi_stream_t stream);
+
+/* ---- gpu_radix_join execution method
+ *      (radix-join/src/execution_methods/gpu_radix_join.rs:90-565) ------ */
+
+/* Result of a whole join: wrapping i64 sum of the matched probe payloads
+ * (what gpu_radix_join returns) and the number of matches. */
+typedef struct {
+  int64_t sum;
+  uint64_t count;
+} fi_join_result;
+
+typedef struct fi_radix_join_engine fi_radix_join_engine;
+
+/* Allocates device workspace for joins of up to max_build x max_probe
+ * tuples of `tuple_bytes`-byte tuples with `radix_bits` (one or two passes)
+ * and `hashing_scheme` (PERFECT or BUCKET_CHAINING). */
+int fi_radix_join_engine_new(uint64_t max_build_len, uint64_t max_probe_len,
+                             uint32_t tuple_bytes, fi_radix_bits radix_bits,
+                             fi_hashing_scheme hashing_scheme,
+                             fi_radix_join_engine **out);
+void fi_radix_join_engine_free(fi_radix_join_engine *e);
+
+/* Device bytes the engine holds. */
+uint64_t fi_radix_join_engine_workspace_bytes(const fi_radix_join_engine *e);
+
+/* gpu_radix_join over device-resident columns: prefix sum, partition (one
+ * or two passes) and per-partition join, all enqueued on `stream`.
+ * `result` is a device fi_join_result that receives the result (it is
+ * overwritten).  Asynchronous. */
+int fi_radix_join_engine_run_int32(fi_radix_join_engine *e,
+                                   const int32_t *build_key,
+                                   const int32_t *build_pay, uint64_t build_len,
+                                   const int32_t *probe_key,
+                                   const int32_t *probe_pay, uint64_t probe_len,
+                                   fi_join_result *result, fi_stream_t stream);
+int fi_radix_join_engine_run_int64(fi_radix_join_engine *e,
+                                   const int64_t *build_key,
+                                   const int64_t *build_pay, uint64_t build_len,
+                                   const int64_t *probe_key,
+                                   const int64_t *probe_pay, uint64_t probe_len,
+                                   fi_join_result *result, fi_stream_t stream);
+
+/* Same join from host memory (ideally pinned): copies the four columns to
+ * the device inside the call, runs the join and copies the result back into
+ * the host `result`.  Synchronous. */
+int fi_radix_join_engine_run_host_int64(fi_radix_join_engine *e,
+                                        const int64_t *build_key,
+                                        const int64_t *build_pay,
+                                        uint64_t build_len,
+                                        const int64_t *probe_key,
+                                        const int64_t *probe_pay,
+                                        uint64_t probe_len,
+                                        fi_join_result *result,
+                                        fi_stream_t stream);
+
+/* Synchronises and reports (and clears) a device-side error of the engine. */
+int fi_radix_join_engine_status(fi_radix_join_engine *e);
+
+/* Phase timing (no reference counterpart; the reference times its phases
+ * with CUDA events in gpu_radix_join.rs:255-276,281-356,415-532).  When
+ * `events` (cudaEvent_t[n_events], n_events >= FI_ENGINE_PHASE_EVENTS) is
+ * set, every run records events[i] on its stream after phase i:
+ *   0 start, then per relation r in {build, probe}: 1+4r pass-1 histogram,
+ *   2+4r pass-1 scatter, 3+4r pass-2 plan + histogram + cursors,
+ *   4+4r pass-2 scatter; 9 join; 10 result.
+ * Pass NULL to stop recording. */
+#define FI_ENGINE_PHASE_EVENTS 11
+int fi_radix_join_engine_set_events(fi_radix_join_engine *e, void **events,
+                                    uint32_t n_events);
+
+/* Number of kernels the last run launched. */
+uint32_t fi_radix_join_engine_last_launches(const fi_radix_join_engine *e);
+
+/* ---- seeded relation generator (datagen/src/relation.rs counterpart) -- */
+
+/* keys[i] = base + perm(i), a seeded permutation of base..base+n-1. */
+int fi_datagen_primary_keys_int32(int32_t *keys, uint64_t n, uint64_t seed,
+                                  int32_t base, fi_stream_t stream);
+int fi_datagen_primary_keys_int64(int64_t *keys, uint64_t n, uint64_t seed,
+                                  int64_t base, fi_stream_t stream);
+/* Uniform foreign keys over base..base+pk_n-1. */
+int fi_datagen_uniform_foreign_keys_int32(int32_t *keys, uint64_t n,
+                                          uint64_t pk_n, uint64_t seed,
+                                          int32_t base, fi_stream_t stream);
+int fi_datagen_uniform_foreign_keys_int64(int64_t *keys, uint64_t n,
+                                          uint64_t pk_n, uint64_t seed,
+                                          int64_t base, fi_stream_t stream);
+/* Zipf(s) ranks over pk_n primary keys generated with pk_seed, mapped to
+ * their keys (s = 0: uniform ranks). */
+int fi_datagen_zipf_foreign_keys_int32(int32_t *keys, uint64_t n,
+                                       uint64_t pk_n, double s, uint64_t seed,
+                                       uint64_t pk_seed, int32_t base,
+                                       fi_stream_t stream);
+int fi_datagen_zipf_foreign_keys_int64(int64_t *keys, uint64_t n,
+                                       uint64_t pk_n, double s, uint64_t seed,
+                                       uint64_t pk_seed, int64_t base,
+                                       fi_stream_t stream);
+/* Uniform 64-bit keys. */
+int fi_datagen_uniform_u64_keys(int64_t *keys, uint64_t n, uint64_t seed,
+                                fi_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FI_SQLOPS_H */

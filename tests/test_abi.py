@@ -1,0 +1,103 @@
+"""CPU checks of the C ABI: the library loads, exports every symbol
+include/fi_sqlops.h declares, and its host-side helpers (no GPU needed) keep
+the reference's layout rules."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(REPO, "include", "fi_sqlops.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fi_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(fi):
+    syms = declared_symbols()
+    assert len(syms) >= 45
+    missing = [s for s in syms if not hasattr(fi.lib(), s)]
+    assert missing == []
+
+
+def test_version(fi):
+    assert b"sm_100a" in fi.lib().fi_version()
+
+
+def test_input_chunk_size(fi, oracle):
+    # partition_input_chunk.rs:24-35
+    for n, c, kb in [(0, 1, 8), (100, 3, 4), (10**6, 148, 8), (2**29, 148, 8),
+                     (2**30 + 7, 148, 4), (77, 80, 8)]:
+        assert fi.input_chunk_size(n, c, kb) == oracle.input_chunk_size(n, c, kb)
+    with pytest.raises(fi.SqlOpsError) as e:
+        fi.input_chunk_size(2**33, 1, 8)
+    assert e.value.kind == "IntegerOverflow"
+
+
+def test_padding_len(fi):
+    assert fi.lib().fi_padding_len(8) == 16
+    assert fi.lib().fi_padding_len(16) == 8
+
+
+def test_partitioned_relation_helpers(fi):
+    lib = fi.lib()
+    rel = fi._RelationC()
+    # Chunked, 4 chunks, 2 bits, int64 tuples: 100 + 4*4*8 padding tuples
+    n_alloc = lib.fi_partitioned_relation_alloc_len(C.c_uint64(100), 0, 2, 4, 16)
+    assert n_alloc == 100 + 4 * 4 * 8
+    with pytest.raises(fi.SqlOpsError):
+        fi._check(lib.fi_partitioned_relation_init(
+            C.byref(rel), C.c_uint64(100), 0, 2, 4, 16, C.c_void_p(1),
+            C.c_uint64(n_alloc - 1), C.c_void_p(2)))
+    fi._check(lib.fi_partitioned_relation_init(
+        C.byref(rel), C.c_uint64(100), 0, 2, 4, 16, C.c_void_p(1),
+        C.c_uint64(n_alloc), C.c_void_p(2)))
+    assert rel.chunks == 4 and rel.len == 100
+    # partition_len over host offsets (partitioned_relation.rs:409-437)
+    import numpy as np
+    pad = 8
+    sizes = np.array([[3, 5, 0, 17], [9, 1, 1, 4], [0, 0, 30, 0], [10, 10, 5, 5]])
+    offs, pos = [], 0
+    for c in range(4):
+        for p in range(4):
+            pos += pad
+            offs.append(pos)
+            pos += sizes[c, p]
+    offs = np.array(offs, np.uint64)
+    rel.len = int(sizes.sum())
+    for p in range(4):
+        out = C.c_uint64(0)
+        fi._check(lib.fi_partition_len(C.byref(rel), C.c_void_p(offs.ctypes.data),
+                                       p, C.byref(out)))
+        assert out.value == sizes[:, p].sum()
+    with pytest.raises(fi.SqlOpsError) as e:
+        fi._check(lib.fi_partition_len(C.byref(rel), C.c_void_p(offs.ctypes.data),
+                                       4, C.byref(C.c_uint64())))
+    assert "Invalid partition ID" in str(e.value)
+    # resize (partitioned_relation.rs:383-395)
+    fi._check(lib.fi_partitioned_relation_resize(C.byref(rel), C.c_uint64(100)))
+    with pytest.raises(fi.SqlOpsError):
+        fi._check(lib.fi_partitioned_relation_resize(C.byref(rel), C.c_uint64(101)))
+
+
+def test_partition_offsets_init(fi):
+    o = fi._OffsetsC()
+    fi._check(fi.lib().fi_partition_offsets_init(C.byref(o), 1, 148, 9, 16,
+                                                 C.c_void_p(8), C.c_void_p(16)))
+    assert o.chunks == 1 and o.max_chunks == 148 and o.local_offsets == 16
+    fi._check(fi.lib().fi_partition_offsets_init(C.byref(o), 0, 148, 9, 16,
+                                                 C.c_void_p(8), C.c_void_p(16)))
+    assert o.chunks == 148 and o.local_offsets is None
+
+
+def test_errors_without_launch(fi):
+    """Argument validation happens on the host before any launch."""
+    with pytest.raises(fi.SqlOpsError) as e:
+        fi.CudaRadixJoin(fi.RadixPass.Second, fi.RadixBits(5), fi.HashingScheme.Perfect,
+                         4, 128)
+    assert e.value.kind == "InvalidArgument"
+    assert "pass is not specified" in str(e.value)

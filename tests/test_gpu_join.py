@@ -1,0 +1,273 @@
+"""GPU parity of the joins against the oracle, through the C ABI.
+
+Radix join: the reference's known-answer tests (test_cuda_radix_join.rs:
+40-365): primary keys 0..N-1 shuffled, foreign keys over them, payload =
+row + 1, so SUM(s.value) = N_s (N_s + 1) / 2; perfect hashing on 6100*2^b
+build tuples and bucket chaining on 4096*2^b, grids of 1, 3 and 80 blocks.
+Plus: sum and match count equal to the oracle's restated join, the task
+assignments equal to the reference's greedy split, Zipf-skewed probes and
+build partitions larger than shared memory.  No-partitioning join: sums equal
+to the reference CPU operators' (golden-pinned oracle).  Engine: the whole
+gpu_radix_join against the oracle on one- and two-pass configurations."""
+import numpy as np
+import pytest
+import torch
+
+from _helpers import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+DTYPES = [(np.int32, torch.int32), (np.int64, torch.int64)]
+
+
+def partition_contiguous(fi, keys, pays, bits, radix_bits=None, pass_=None,
+                         hist="Chunked"):
+    """One contiguous relation as the reference join tests build it
+    (Chunked with num_chunks = 1)."""
+    tdt = keys.dtype
+    radix_bits = radix_bits or fi.RadixBits(bits)
+    pass_ = fi.RadixPass.First if pass_ is None else pass_
+    H = getattr(fi.GpuHistogramAlgorithm, hist)
+    p = fi.GpuRadixPartitioner(H, fi.GpuRadixPartitionAlgorithm.NC, radix_bits, 1, 1024)
+    o = fi.PartitionOffsets(H, 1, bits, tdt)
+    rel = fi.PartitionedRelation(keys.numel(), H, bits, 1, tdt, fill=-1)
+    p.prefix_sum(pass_, keys, o)
+    p.partition(pass_, keys, pays, o, rel)
+    return rel
+
+
+def gen_join(oracle, n_build, n_probe, dt, seed, zipf=None):
+    r_key = oracle.primary_keys(n_build, seed, dt, base=0)
+    if zipf is None:
+        s_key = oracle.uniform_foreign_keys(n_probe, n_build, seed + 1, dt, base=0)
+    else:
+        s_key = oracle.zipf_foreign_keys(n_probe, n_build, zipf, seed + 1, seed, dt,
+                                         base=0)
+    r_pay = np.arange(1, n_build + 1, dtype=dt)
+    s_pay = np.arange(1, n_probe + 1, dtype=dt)
+    return r_key, r_pay, s_key, s_pay
+
+
+JOIN_CASES = [("Perfect", 0, 6100), ("Perfect", 4, 6100 * 16), ("Perfect", 8, 6100 * 256),
+              ("BucketChaining", 0, 4096), ("BucketChaining", 3, 4096 * 8),
+              ("BucketChaining", 8, 4096 * 256)]
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme,bits,n", JOIN_CASES)
+@pytest.mark.parametrize("grid,block", [(1, 128), (3, 256), (80, 1024)])
+def test_radix_join_known_answer(fi, oracle, ndt, tdt, scheme, bits, n, grid, block):
+    r_key, r_pay, s_key, s_pay = gen_join(oracle, n, n, ndt, 10 + bits)
+    b = partition_contiguous(fi, to_dev(r_key), to_dev(r_pay), bits)
+    pr = partition_contiguous(fi, to_dev(s_key), to_dev(s_pay), bits)
+    result = torch.zeros(grid * block, dtype=torch.int64, device="cuda")
+    tasks = torch.zeros(grid + 1, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    j = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(bits),
+                         getattr(fi.HashingScheme, scheme), grid, block)
+    j.join(b, pr, result, tasks, match_count=count)
+    j.status()
+    assert int(to_host(result).sum()) == n * (n + 1) // 2
+    assert int(to_host(count)[0]) == n
+    # task assignments as the reference's greedy split (radix_join.cu:58-98)
+    exp_tasks = oracle.assign_tasks(to_host(pr.offsets).astype(np.uint64),
+                                    pr.padded_len(), pr.padding_len(), bits, grid,
+                                    ndt)
+    np.testing.assert_array_equal(to_host(tasks).astype(np.uint32), exp_tasks)
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["Perfect", "BucketChaining"])
+@pytest.mark.parametrize("zipf", [None, 0.5, 1.0, 1.5])
+def test_radix_join_matches_oracle(fi, oracle, ndt, tdt, scheme, zipf):
+    bits, n_b, n_p = 7, 300000, 700001
+    r_key, r_pay, s_key, _ = gen_join(oracle, n_b, n_p, ndt, 31, zipf=zipf)
+    s_pay = oracle.uniform_foreign_keys(n_p, 1 << 30, 77, ndt) - (1 << 29)
+    b = partition_contiguous(fi, to_dev(r_key), to_dev(r_pay), bits)
+    pr = partition_contiguous(fi, to_dev(s_key), to_dev(s_pay.astype(ndt)), bits)
+    grid, block = 148, 1024
+    result = torch.zeros(grid * block, dtype=torch.int64, device="cuda")
+    tasks = torch.zeros(grid + 1, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    j = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(bits),
+                         getattr(fi.HashingScheme, scheme), grid, block)
+    j.join(b, pr, result, tasks, match_count=count)
+    j.status()
+    bh, ph = to_host(b.relation), to_host(pr.relation)
+    s, c = oracle.radix_join("chaining" if scheme == "BucketChaining" else "perfect",
+                             bh[:b.padded_len()], to_host(b.offsets).astype(np.uint64),
+                             b.padding_len(), ph[:pr.padded_len()],
+                             to_host(pr.offsets).astype(np.uint64), pr.padding_len(),
+                             bits, bits, ht_entries=1 << 20)
+    got = int(to_host(result).astype(np.int64).sum(dtype=np.int64))
+    assert got == s
+    assert int(to_host(count)[0]) == c == n_p
+
+
+def test_radix_join_build_larger_than_shared_memory(fi, oracle):
+    """One partition of 200K build tuples: joined in shared-memory rounds
+    (the reference asserts on this size, radix_join.cu:251-252)."""
+    n = 200000
+    r_key, r_pay, s_key, s_pay = gen_join(oracle, n, n, np.int64, 5)
+    b = partition_contiguous(fi, to_dev(r_key), to_dev(r_pay), 0)
+    pr = partition_contiguous(fi, to_dev(s_key), to_dev(s_pay), 0)
+    result = torch.zeros(148 * 1024, dtype=torch.int64, device="cuda")
+    tasks = torch.zeros(149, dtype=torch.int32, device="cuda")
+    j = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(0),
+                         fi.HashingScheme.BucketChaining, 148, 1024)
+    j.join(b, pr, result, tasks)
+    j.status()
+    assert int(to_host(result).sum()) == n * (n + 1) // 2
+
+
+def test_radix_join_second_pass_relations(fi, oracle):
+    """A join on second-pass relations (ignore bits = first + second pass
+    bits, cuda_radix_join.rs:207-208)."""
+    n, b1, b2 = 100000, 3, 5
+    r_key, r_pay, s_key, s_pay = gen_join(oracle, n, n, np.int64, 6)
+    bits = fi.RadixBits(b1, b2)
+    # every key of one first-pass partition: keys with low b1 bits == 2
+    rk, rp = r_key[(r_key & 7) == 2], r_pay[(r_key & 7) == 2]
+    sk, sp = s_key[(s_key & 7) == 2], s_pay[(s_key & 7) == 2]
+    b = partition_contiguous(fi, to_dev(rk), to_dev(rp), b2, bits, fi.RadixPass.Second)
+    pr = partition_contiguous(fi, to_dev(sk), to_dev(sp), b2, bits, fi.RadixPass.Second)
+    result = torch.zeros(10 * 256, dtype=torch.int64, device="cuda")
+    tasks = torch.zeros(11, dtype=torch.int32, device="cuda")
+    for scheme in (fi.HashingScheme.Perfect, fi.HashingScheme.BucketChaining):
+        result.zero_()
+        j = fi.CudaRadixJoin(fi.RadixPass.Second, bits, scheme, 10, 256)
+        j.join(b, pr, result, tasks)
+        j.status()
+        assert int(to_host(result).sum()) == int(sp.sum())
+
+
+def test_radix_join_validation(fi):
+    rel = fi.PartitionedRelation(10, fi.GpuHistogramAlgorithm.Chunked, 2, 4, torch.int64)
+    one = fi.PartitionedRelation(10, fi.GpuHistogramAlgorithm.Chunked, 2, 1, torch.int64)
+    j = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(2), fi.HashingScheme.Perfect,
+                         4, 128)
+    res = torch.zeros(512, dtype=torch.int64, device="cuda")
+    with pytest.raises(fi.SqlOpsError, match="Chunked build relations"):
+        j.join(rel, one, res, torch.zeros(5, dtype=torch.int32, device="cuda"))
+    with pytest.raises(fi.SqlOpsError, match="grid size \\+ 1"):
+        j.join(one, one, res, torch.zeros(4, dtype=torch.int32, device="cuda"))
+    lp = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(2),
+                          fi.HashingScheme.LinearProbing, 4, 128)
+    with pytest.raises(fi.SqlOpsError) as e:
+        lp.join(one, one, res, torch.zeros(5, dtype=torch.int32, device="cuda"))
+    assert e.value.kind == "Unsupported"
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["LinearProbing", "Perfect"])
+def test_hash_join(fi, oracle, ndt, tdt, scheme):
+    n_b, n_p = 100003, 300007
+    r_key = oracle.primary_keys(n_b, 3, ndt, base=0)
+    r_pay = oracle.uniform_foreign_keys(n_b, 1000, 4, ndt)
+    s_key = oracle.uniform_foreign_keys(n_p, n_b + 500, 5, ndt, base=0)
+    s_pay = oracle.uniform_foreign_keys(n_p, 1 << 20, 6, ndt)
+    size = (1 << 18) if scheme == "LinearProbing" else n_b + 500
+    ht = fi.HashTable(size, tdt)
+    hj = fi.CudaHashJoin(getattr(fi.HashingScheme, scheme), ht, (148, 512), (148, 512))
+    hj.build(to_dev(r_key), to_dev(r_pay))
+    res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
+    hj.probe_sum(to_dev(s_key), to_dev(s_pay), res)
+    got = int(to_host(res).astype(np.uint64).sum(dtype=np.uint64))
+    if scheme == "LinearProbing":
+        exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    else:
+        exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got == exp
+
+
+def test_hash_join_selective_perfect(fi, oracle):
+    n = 50000
+    r_key = oracle.primary_keys(n, 3, np.int64, base=0)
+    r_key[::7] = -1  # null keys are skipped by the selective build
+    r_pay = np.arange(n, dtype=np.int64)
+    s_key = oracle.uniform_foreign_keys(n, n, 5, np.int64, base=0)
+    s_pay = np.ones(n, np.int64)
+    ht = fi.HashTable(n, torch.int64)
+    hj = fi.CudaHashJoin(fi.HashingScheme.Perfect, ht, (20, 256), (20, 256),
+                         is_selective=True)
+    hj.build(to_dev(r_key), to_dev(r_pay))
+    res = torch.zeros(20 * 256, dtype=torch.int64, device="cuda")
+    hj.probe_sum(to_dev(s_key), to_dev(s_pay), res)
+    exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, n, selective=True)
+    assert int(to_host(res).sum()) == exp
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("bits,scheme", [((10, None), "BucketChaining"),
+                                         ((6, 6), "Perfect"),
+                                         ((9, 9), "BucketChaining"),
+                                         ((9, 9), "Perfect")])
+def test_engine_matches_oracle(fi, oracle, ndt, tdt, bits, scheme):
+    n_b, n_p = 1 << 21, (1 << 21) + 12345
+    r_key = oracle.primary_keys(n_b, 41, ndt)
+    r_pay = r_key.copy()
+    s_key = oracle.uniform_foreign_keys(n_p, n_b, 42, ndt)
+    s_pay = s_key.copy()
+    e = fi.RadixJoinEngine(n_b, n_p, tdt, fi.RadixBits(*bits),
+                           getattr(fi.HashingScheme, scheme))
+    s, c = e.run(to_dev(r_key), to_dev(r_pay), to_dev(s_key), to_dev(s_pay))
+    e.status()
+    b1 = bits[0]
+    b2 = bits[1] or 0
+    exp_s, exp_c, _, _ = oracle.cpu_radix_join(
+        r_key.astype(np.int64), r_pay.astype(np.int64), s_key.astype(np.int64),
+        s_pay.astype(np.int64), b1, max(b2, 1), 8, use_reference=False)
+    assert c == exp_c == n_p
+    assert s == exp_s
+
+
+@pytest.mark.parametrize("zipf", [0.0, 0.5, 1.0, 1.5])
+def test_engine_zipf_closed_form(fi, oracle, zipf):
+    """All S keys are foreign keys: count = |S|, sum = sum(S.payload)."""
+    n = 1 << 22
+    rk = torch.empty(n, dtype=torch.int64, device="cuda")
+    sk = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_primary_keys(rk, 1)
+    fi.gen_zipf_foreign_keys(sk, n, zipf, 2, 1)
+    e = fi.RadixJoinEngine(n, n, torch.int64, fi.RadixBits(9, 9),
+                           fi.HashingScheme.BucketChaining)
+    s, c = e.run(rk, rk, sk, sk)
+    e.status()
+    assert c == n
+    assert s == int(sk.sum().item())
+
+
+def test_engine_int32_config1_bit_exact(fi, oracle):
+    """Config 1 (16M x 16M int32, 10 bits, one pass, bucket chaining, payload
+    = key) against the CPU radix join."""
+    n = 16 << 20
+    r_key = oracle.primary_keys(n, 101, np.int32)
+    s_key = oracle.uniform_foreign_keys(n, n, 102, np.int32)
+    e = fi.RadixJoinEngine(n, n, torch.int32, fi.RadixBits(10),
+                           fi.HashingScheme.BucketChaining)
+    s, c = e.run(to_dev(r_key), to_dev(r_key), to_dev(s_key), to_dev(s_key))
+    e.status()
+    exp_s, exp_c, _, _ = oracle.cpu_radix_join(
+        r_key.astype(np.int64), r_key.astype(np.int64), s_key.astype(np.int64),
+        s_key.astype(np.int64), 10, 1, 8, use_reference=False)
+    assert (s, c) == (exp_s, exp_c)
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+def test_gpu_generator_matches_cpu(fi, oracle, ndt, tdt):
+    n = 1 << 20
+    pk = torch.empty(n, dtype=tdt, device="cuda")
+    fi.gen_primary_keys(pk, 7, base=1)
+    np.testing.assert_array_equal(to_host(pk), oracle.primary_keys(n, 7, ndt, base=1))
+    fk = torch.empty(n, dtype=tdt, device="cuda")
+    fi.gen_uniform_foreign_keys(fk, 12345, 9, base=1)
+    np.testing.assert_array_equal(to_host(fk),
+                                  oracle.uniform_foreign_keys(n, 12345, 9, ndt, base=1))
+    if ndt == np.int64:
+        u = torch.empty(n, dtype=tdt, device="cuda")
+        fi.gen_uniform_u64_keys(u, 3)
+        np.testing.assert_array_equal(to_host(u), oracle.uniform_u64_keys(n, 3))
+    z = torch.empty(n, dtype=tdt, device="cuda")
+    fi.gen_zipf_foreign_keys(z, 100000, 1.5, 4, 9)
+    zc = oracle.zipf_foreign_keys(n, 100000, 1.5, 4, 9, ndt)
+    assert (to_host(z) == zc).mean() > 0.999
