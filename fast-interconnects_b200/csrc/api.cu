@@ -652,12 +652,12 @@ struct fi_cuda_radix_join {
   int32_t bits[3];
   fi_hashing_scheme scheme;
   uint32_t grid, block;
-  DevBuf item_start, counters, tile_state, status;
+  DevBuf item_start, item_part, counters, tile_state, status;
 
   JoinScratch js() {
-    uint32_t *c = (uint32_t *)counters.ptr;
-    return JoinScratch{(uint32_t *)item_start.ptr, c, (uint64_t *)tile_state.ptr,
-                       c + 1, (int *)status.ptr};
+    return JoinScratch{(uint32_t *)item_start.ptr, (uint32_t *)item_part.ptr,
+                       (uint64_t *)tile_state.ptr, (uint32_t *)counters.ptr,
+                       (int *)status.ptr};
   }
 };
 
@@ -691,6 +691,7 @@ extern "C" int fi_cuda_radix_join_new(fi_radix_pass radix_pass,
 extern "C" void fi_cuda_radix_join_free(fi_cuda_radix_join *j) {
   if (!j) return;
   j->item_start.release();
+  j->item_part.release();
   j->counters.release();
   j->tile_state.release();
   j->status.release();
@@ -737,6 +738,9 @@ static int radix_join_impl(fi_cuda_radix_join *j,
                      "PartitionedRelation has mismatching radix bits");
   const uint32_t F = 1u << bits;
   int rc = j->item_start.reserve((size_t)(F + 1) * sizeof(uint32_t), false);
+  if (rc) return rc;
+  rc = j->item_part.reserve(
+      (size_t)join_items_capacity(F, rel_padded_len(pr)) * sizeof(uint32_t), false);
   if (rc) return rc;
   rc = j->counters.reserve(4 * sizeof(uint32_t), true);
   if (rc) return rc;

@@ -10,15 +10,17 @@
 // B200 design:
 //  * Work items instead of static partition ranges: every partition whose
 //    build and probe sides are both non-empty becomes ceil(|S_p| / W) items
-//    (W probe tuples each).  A planning kernel counts the items and scans
-//    them (decoupled look-back).  Persistent CTAs take items from an atomic
-//    counter, so a Zipf-skewed partition is probed by many CTAs instead of
-//    one, and CTAs never idle while work is left.
-//  * The build side of an item's partition is loaded into shared memory (up
-//    to the 227 KB opt-in size): a bucket-chaining table (heads + next links
-//    + keys) or a perfect-hash array indexed by key >> ignore_bits.  A CTA
-//    keeps its table when its next item belongs to the same partition.
-//    Build values are not stored: the aggregate only reads s.value.
+//    (W probe tuples each).  A planning kernel counts the items, scans them
+//    (decoupled look-back) and writes an item -> partition table.  Persistent
+//    CTAs walk the items with a grid stride, so a Zipf-skewed partition is
+//    probed by many CTAs instead of one.
+//  * The build side of an item's partition is loaded into shared memory: a
+//    bucket-chaining table (u32 heads, u16 next links, keys) sized from the
+//    average build partition, or a perfect-hash array indexed by
+//    key >> ignore_bits.  With blocks of up to 512 threads two CTAs share an
+//    SM, so one CTA's build overlaps the other's probe.  A CTA keeps its
+//    table when its next item belongs to the same partition.  Build values
+//    are not stored: the aggregate only reads s.value.
 //  * A build side larger than the table is joined in rounds (each round
 //    builds a slice and probes the item), so capacity is never exceeded
 //    (the reference asserts instead).
@@ -34,9 +36,6 @@ namespace fi {
 
 constexpr uint32_t kPlanThreads = 1024;
 constexpr uint32_t kProbeUnroll = 4;
-constexpr uint32_t kChainLog2Buckets = 13;  // 8192 buckets
-constexpr uint32_t kEnd = 0xffffffffu;
-constexpr uint32_t kCtrlSmem = 256;  // bytes reserved for control variables
 
 // ---- reference greedy task assignment --------------------------------------
 // Same result as gpu_radix_join_assign_tasks (radix_join.cu:58-98), with the
@@ -102,8 +101,8 @@ __global__ void __launch_bounds__(kPlanThreads)
                      uint32_t build_pad, const uint64_t *__restrict__ probe_off,
                      uint64_t probe_len, uint32_t probe_pad, uint32_t F,
                      uint32_t width, uint32_t *__restrict__ item_start,
-                     uint64_t *tile_state, uint32_t *tile_counter,
-                     int *status) {
+                     uint32_t *__restrict__ item_part, uint64_t *tile_state,
+                     uint32_t *tile_counter, int *status) {
   __shared__ uint32_t tile_s, prefix_s;
   __shared__ uint32_t warp_tmp[33];
   __shared__ uint32_t vals[kPlanThreads];
@@ -152,26 +151,26 @@ __global__ void __launch_bounds__(kPlanThreads)
     prefix_s = (uint32_t)prefix;
   }
   __syncthreads();
-  if (p < F) item_start[p] = prefix_s + vals[threadIdx.x];
+  if (p < F) {
+    const uint32_t first = prefix_s + vals[threadIdx.x];
+    item_start[p] = first;
+    for (uint32_t k = 0; k < items; ++k) item_part[first + k] = p;
+  }
   if (p + 1 == F) item_start[F] = prefix_s + vals[threadIdx.x] + items;
 }
 
 // ---- the join -------------------------------------------------------------
-template <typename K>
-struct ChainTable {
-  uint32_t *heads;  // [1 << kChainLog2Buckets]
-  uint32_t *next;   // [cap]
-  K *keys;          // [cap]
-  uint32_t cap;
-};
+constexpr uint32_t kLinkEnd = 0xffffu;  // u16 chain links
+constexpr uint32_t kHeadEnd = 0xffffffffu;
 
 template <typename K>
-__device__ __forceinline__ uint32_t chain_bucket(K key, uint32_t ignore_bits) {
+__device__ __forceinline__ uint32_t chain_bucket(K key, uint32_t ignore_bits,
+                                                 uint32_t log2_buckets) {
   // hash of the key bits above the partition bits (radix_join.cu:275-276)
   return mult_shift_hash<K>(
       static_cast<K>(static_cast<uint64_t>(static_cast<int64_t>(key)) >>
                      ignore_bits),
-      kChainLog2Buckets);
+      log2_buckets);
 }
 
 template <typename K>
@@ -179,65 +178,73 @@ __device__ __forceinline__ uint64_t perfect_index(K key, uint32_t ignore_bits) {
   return static_cast<uint64_t>(static_cast<int64_t>(key)) >> ignore_bits;
 }
 
-template <typename K, int kScheme>
-__global__ void __launch_bounds__(1024, 1) radix_join_kernel(
+// Table layout in dynamic shared memory.
+//   chaining: keys K[cap] | next u16[cap] | heads u32[2^log2_buckets]
+//   perfect:  keys K[pcap], indexed by key >> ignore_bits
+template <typename K>
+struct SmemTable {
+  K *keys;
+  uint16_t *next;
+  uint32_t *heads;
+  uint32_t cap;
+};
+
+template <typename K>
+__host__ __device__ inline uint32_t chain_capacity(uint32_t table_bytes,
+                                                   uint32_t log2_buckets) {
+  const uint32_t hb = 4u << log2_buckets;
+  if (table_bytes <= hb + 64) return 0;
+  uint32_t cap = (table_bytes - hb - 64) / (uint32_t)(sizeof(K) + 2);
+  cap &= ~7u;
+  return cap < 65528u ? cap : 65528u;
+}
+
+// Persistent join: CTA b takes items b, b + grid, b + 2*grid, ...  Items
+// are near-equal in probe work (at most `width` probe tuples each), so the
+// grid stride balances skewed inputs while avoiding a global work counter;
+// the partition of the next item is prefetched.
+template <typename K, int kScheme, int kMaxThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
     const Tuple<K> *__restrict__ build, const uint64_t *__restrict__ build_off,
     uint64_t build_len, uint32_t build_pad, const Tuple<K> *__restrict__ probe,
     const uint64_t *__restrict__ probe_off, uint64_t probe_len,
     uint32_t probe_pad, uint32_t F, uint32_t ignore_bits,
-    const uint32_t *__restrict__ item_start, uint32_t *item_counter,
-    uint32_t smem_bytes, int64_t *__restrict__ result_set,
+    const uint32_t *__restrict__ item_start,
+    const uint32_t *__restrict__ item_part, uint32_t table_bytes,
+    uint32_t log2_buckets, int64_t *__restrict__ result_set,
     uint64_t *match_count, int *status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t *ctrl = reinterpret_cast<uint32_t *>(smem_raw);  // item, p, max
-  unsigned char *table = smem_raw + kCtrlSmem;
-  const uint32_t table_bytes = smem_bytes - kCtrlSmem;
+  __shared__ uint32_t s_used;
+  __shared__ uint64_t red_tmp[32];
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
 
-  // table layout
-  ChainTable<K> ct;
-  K *pkeys = reinterpret_cast<K *>(table);
-  uint32_t pcap = 0;
+  SmemTable<K> tb;
+  tb.keys = reinterpret_cast<K *>(smem_raw);
+  uint32_t cap, pcap = 0;
   if (kScheme == 2) {
-    const uint32_t nb = 1u << kChainLog2Buckets;
-    ct.heads = reinterpret_cast<uint32_t *>(table);
-    ct.cap = (table_bytes - nb * 4u) / (uint32_t)(sizeof(K) + 4u);
-    ct.keys = reinterpret_cast<K *>(table + nb * 4u);
-    ct.next = reinterpret_cast<uint32_t *>(table + nb * 4u + ct.cap * sizeof(K));
+    cap = chain_capacity<K>(table_bytes, log2_buckets);
+    tb.next = reinterpret_cast<uint16_t *>(tb.keys + cap);
+    tb.heads = reinterpret_cast<uint32_t *>(smem_raw +
+                                            ((cap * (sizeof(K) + 2) + 15) & ~15u));
   } else {
     pcap = table_bytes / (uint32_t)sizeof(K);
+    cap = 0xffffffffu;
+    // every slot starts empty; afterwards only the used prefix is cleared
+    for (uint32_t i = tid; i < pcap; i += nt) tb.keys[i] = null_key<K>();
   }
-  const uint32_t cap = (kScheme == 2) ? ct.cap : 0xffffffffu;
-  if (kScheme != 2) {
-    // every slot starts empty; afterwards only used slots are cleared
-    for (uint32_t i = threadIdx.x; i < pcap; i += blockDim.x)
-      pkeys[i] = null_key<K>();
-  }
+  const uint32_t nbuckets = 1u << log2_buckets;
 
   const uint32_t total_items = item_start[F];
   int64_t sum = 0;
   uint64_t cnt = 0;
   int64_t cached_p = -1;
-  uint64_t cached_used = 0;  // perfect: highest slot written + 1
+  uint32_t cached_used = 0;  // perfect: highest slot written + 1
 
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t item = atomicAdd(item_counter, 1u);
-      uint32_t p = 0;
-      if (item < total_items) {
-        uint32_t lo = 0, hi = F;  // last p with item_start[p] <= item
-        while (hi - lo > 1) {
-          uint32_t mid = (lo + hi) >> 1;
-          if (item_start[mid] <= item) lo = mid; else hi = mid;
-        }
-        p = lo;
-      }
-      ctrl[0] = item;
-      ctrl[1] = p;
-    }
-    __syncthreads();
-    const uint32_t item = ctrl[0], p = ctrl[1];
-    if (item >= total_items) break;
+  uint32_t item = blockIdx.x;
+  uint32_t p = item < total_items ? item_part[item] : 0u;
+  for (; item < total_items; item += gridDim.x) {
+    const uint32_t nitem = item + gridDim.x;
+    const uint32_t np = nitem < total_items ? item_part[nitem] : 0u;  // prefetch
     const uint32_t k = item - item_start[p];
     const uint32_t nitems = item_start[p + 1] - item_start[p];
     uint64_t bb, be, pb, pe;
@@ -248,93 +255,105 @@ __global__ void __launch_bounds__(1024, 1) radix_join_kernel(
     const uint64_t bsize = be - bb;
 
     for (uint64_t r0 = 0; r0 < bsize; r0 += cap) {
-      const uint64_t rn = min((uint64_t)cap, bsize - r0);
+      const uint32_t rn = (uint32_t)min((uint64_t)cap, bsize - r0);
       const bool reuse = (cached_p == (int64_t)p) && bsize <= cap;
       if (!reuse) {
-        // ---- build ----
+        __syncthreads();  // the previous item's probe is done with the table
         if (kScheme == 2) {
-          for (uint32_t i = threadIdx.x; i < (1u << kChainLog2Buckets);
-               i += blockDim.x)
-            ct.heads[i] = kEnd;
+          for (uint32_t i = tid; i < nbuckets; i += nt) tb.heads[i] = kHeadEnd;
           __syncthreads();
-          for (uint32_t i = threadIdx.x; i < rn; i += blockDim.x) {
-            const K key = load_tuple(build + bb + r0 + i).key;
-            ct.keys[i] = key;
-            ct.next[i] = atomicExch(&ct.heads[chain_bucket(key, ignore_bits)], i);
+          for (uint32_t i0 = 0; i0 < rn; i0 += nt * 4u) {
+            K kk[4];
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+              const uint32_t i = i0 + u * nt + tid;
+              if (i < rn) kk[u] = build[bb + r0 + i].key;
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+              const uint32_t i = i0 + u * nt + tid;
+              if (i < rn) {
+                tb.keys[i] = kk[u];
+                const uint32_t old = atomicExch(
+                    &tb.heads[chain_bucket(kk[u], ignore_bits, log2_buckets)], i);
+                tb.next[i] = (uint16_t)(old == kHeadEnd ? kLinkEnd : old);
+              }
+            }
           }
         } else {
-          // clear the slots the previous build used
-          for (uint64_t i = threadIdx.x; i < cached_used; i += blockDim.x)
-            pkeys[i] = null_key<K>();
+          for (uint32_t i = tid; i < cached_used; i += nt) tb.keys[i] = null_key<K>();
+          if (tid == 0) s_used = 0;
           __syncthreads();
           uint32_t used = 0;
-          for (uint32_t i = threadIdx.x; i < rn; i += blockDim.x) {
-            const K key = load_tuple(build + bb + r0 + i).key;
+          for (uint32_t i = tid; i < rn; i += nt) {
+            const K key = build[bb + r0 + i].key;
             const uint64_t idx = perfect_index(key, ignore_bits);
             if (idx < pcap) {
-              pkeys[idx] = key;
+              tb.keys[idx] = key;
               used = max(used, (uint32_t)idx + 1u);
             } else {
               record_error(status, kDevErrCapacity);
             }
           }
-          // block max of `used`
-          __syncthreads();
-          if (threadIdx.x == 0) ctrl[2] = 0;
-          __syncthreads();
-          atomicMax(&ctrl[2], used);
-          __syncthreads();
-          cached_used = ctrl[2];
+          if (used) atomicMax(&s_used, used);
         }
         __syncthreads();
+        if (kScheme != 2) cached_used = s_used;
         cached_p = (bsize <= cap) ? (int64_t)p : -1;
       }
       // ---- probe ----
-      for (uint64_t base = qb; base < qe;
-           base += (uint64_t)blockDim.x * kProbeUnroll) {
+      for (uint64_t base = qb; base < qe; base += (uint64_t)nt * kProbeUnroll) {
         Tuple<K> t[kProbeUnroll];
 #pragma unroll
         for (uint32_t u = 0; u < kProbeUnroll; ++u) {
-          const uint64_t j = base + (uint64_t)u * blockDim.x + threadIdx.x;
+          const uint64_t j = base + (uint64_t)u * nt + tid;
           if (j < qe) t[u] = load_tuple_cs(probe + j);
         }
 #pragma unroll
         for (uint32_t u = 0; u < kProbeUnroll; ++u) {
-          const uint64_t j = base + (uint64_t)u * blockDim.x + threadIdx.x;
+          const uint64_t j = base + (uint64_t)u * nt + tid;
           if (j >= qe) continue;
           const K key = t[u].key;
           if (kScheme == 2) {
-            for (uint32_t e = ct.heads[chain_bucket(key, ignore_bits)];
-                 e != kEnd; e = ct.next[e]) {
-              if (ct.keys[e] == key) {
-                sum += static_cast<int64_t>(t[u].value);
-                cnt += 1;
+            uint32_t e = tb.heads[chain_bucket(key, ignore_bits, log2_buckets)];
+            if (e != kHeadEnd) {
+              for (;;) {
+                if (tb.keys[e] == key) {
+                  sum += static_cast<int64_t>(t[u].value);
+                  cnt += 1;
+                }
+                const uint32_t nx = tb.next[e];
+                if (nx == kLinkEnd) break;
+                e = nx;
               }
             }
           } else {
             const uint64_t idx = perfect_index(key, ignore_bits);
-            if (idx < pcap && pkeys[idx] == key) {
+            if (idx < pcap && tb.keys[idx] == key) {
               sum += static_cast<int64_t>(t[u].value);
               cnt += 1;
             }
           }
         }
       }
-      if (bsize > cap) __syncthreads();  // next round rebuilds the table
     }
+    p = np;
   }
 
-  result_set[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] += sum;
+  result_set[(uint64_t)blockIdx.x * nt + tid] += sum;
   if (match_count != nullptr) {
-    __shared__ uint64_t red_tmp[32];
-    uint64_t bc = block_reduce_u64(cnt, red_tmp);
-    if (threadIdx.x == 0 && bc != 0) atomicAdd((unsigned long long *)match_count,
-                                               (unsigned long long)bc);
+    const uint64_t bc = block_reduce_u64(cnt, red_tmp);
+    if (tid == 0 && bc != 0)
+      atomicAdd((unsigned long long *)match_count, (unsigned long long)bc);
   }
 }
 
 // ---- launchers ---------------------------------------------------------------
-uint32_t join_items_capacity(uint32_t fanout) { return fanout + 1; }
+constexpr uint64_t kMinItemWidth = 8192;
+
+uint32_t join_items_capacity(uint32_t fanout, uint64_t probe_len) {
+  return (uint32_t)(fanout + probe_len / kMinItemWidth + 2);
+}
 
 template <typename K>
 cudaError_t launch_assign_tasks(const uint64_t *probe_offsets,
@@ -344,6 +363,12 @@ cudaError_t launch_assign_tasks(const uint64_t *probe_offsets,
   assign_tasks_kernel<<<1, 1024, 0, stream>>>(
       probe_offsets, probe_len, probe_pad, 1u << radix_bits, grid, tasks);
   return cudaGetLastError();
+}
+
+template <typename K, int kScheme>
+static const void *join_kernel_ptr(bool two_per_sm) {
+  return two_per_sm ? (const void *)radix_join_kernel<K, kScheme, 512, 2>
+                    : (const void *)radix_join_kernel<K, kScheme, 1024, 1>;
 }
 
 template <typename K>
@@ -356,12 +381,13 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
                               int64_t *result_set, uint64_t *match_count,
                               JoinScratch s, uint32_t sm_count,
                               cudaStream_t stream) {
-  // probe width per item: enough items to keep every CTA busy, but at least
-  // 8K tuples so that table builds stay amortised
+  (void)sm_count;
+  // probe width per item: about four items per CTA for the bulk, never below
+  // kMinItemWidth tuples so that table builds stay amortised
   const uint64_t probe_tuples =
       probe_len > (uint64_t)probe_pad * fanout ? probe_len - (uint64_t)probe_pad * fanout : 0;
-  uint64_t width = probe_tuples / ((uint64_t)grid * 8u + 1u);
-  if (width < 8192) width = 8192;
+  uint64_t width = probe_tuples / ((uint64_t)grid * 4u + 1u);
+  if (width < kMinItemWidth) width = kMinItemWidth;
   if (width > (1u << 30)) width = 1u << 30;
   const uint32_t tiles = (fanout + kPlanThreads - 1) / kPlanThreads;
   cudaError_t e = cudaMemsetAsync(s.tile_state, 0,
@@ -369,33 +395,54 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(s.tile_counter, 0, sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(s.item_counter, 0, sizeof(uint32_t), stream);
-  if (e != cudaSuccess) return e;
   join_plan_kernel<<<tiles, kPlanThreads, 0, stream>>>(
       build_off, build_len, build_pad, probe_off, probe_len, probe_pad, fanout,
-      (uint32_t)width, s.item_start, s.tile_state, s.tile_counter, s.status);
+      (uint32_t)width, s.item_start, s.item_part, s.tile_state, s.tile_counter,
+      s.status);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
-  const uint32_t smem = (uint32_t)device_max_smem_optin();
-  const void *fn = scheme == 2 ? (const void *)radix_join_kernel<K, 2>
-                               : (const void *)radix_join_kernel<K, 0>;
-  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+  // Two CTAs per SM (half the shared memory each) when the block allows it,
+  // so that one CTA's table build overlaps the other's probe.
+  const bool two = block <= 512;
+  const void *fn = scheme == 2 ? join_kernel_ptr<K, 2>(two) : join_kernel_ptr<K, 0>(two);
+  cudaFuncAttributes attr;
+  e = cudaFuncGetAttributes(&attr, fn);
   if (e != cudaSuccess) return e;
-  if (scheme == 2)
-    radix_join_kernel<K, 2><<<grid, block, smem, stream>>>(
-        reinterpret_cast<const Tuple<K> *>(build), build_off, build_len,
-        build_pad, reinterpret_cast<const Tuple<K> *>(probe), probe_off,
-        probe_len, probe_pad, fanout, ignore_bits, s.item_start,
-        s.item_counter, smem, result_set, match_count, s.status);
-  else
-    radix_join_kernel<K, 0><<<grid, block, smem, stream>>>(
-        reinterpret_cast<const Tuple<K> *>(build), build_off, build_len,
-        build_pad, reinterpret_cast<const Tuple<K> *>(probe), probe_off,
-        probe_len, probe_pad, fanout, ignore_bits, s.item_start,
-        s.item_counter, smem, result_set, match_count, s.status);
-  (void)sm_count;
+  int dev = 0, per_sm = 0, reserved = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  uint32_t dyn = (uint32_t)device_max_smem_optin() - (uint32_t)attr.sharedSizeBytes;
+  if (two) {
+    const int half = per_sm / 2 - reserved - (int)attr.sharedSizeBytes;
+    if (half > 0 && (uint32_t)half < dyn) dyn = (uint32_t)half;
+  }
+  dyn &= ~127u;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+
+  // buckets: next power of two above the average build partition
+  const uint64_t build_tuples =
+      build_len > (uint64_t)build_pad * fanout ? build_len - (uint64_t)build_pad * fanout : 0;
+  const uint64_t avg = build_tuples / fanout + 1;
+  uint32_t lb = 8;
+  while (lb < 14 && (1ull << lb) < avg) ++lb;
+  while (lb > 8 && chain_capacity<K>(dyn, lb) < 2 * avg) --lb;
+
+  const auto *b = reinterpret_cast<const Tuple<K> *>(build);
+  const auto *pr = reinterpret_cast<const Tuple<K> *>(probe);
+#define FI_JOIN_LAUNCH(S, T, M)                                                \
+  radix_join_kernel<K, S, T, M><<<grid, block, dyn, stream>>>(                 \
+      b, build_off, build_len, build_pad, pr, probe_off, probe_len, probe_pad, \
+      fanout, ignore_bits, s.item_start, s.item_part, dyn, lb, result_set,     \
+      match_count, s.status)
+  if (scheme == 2) {
+    if (two) FI_JOIN_LAUNCH(2, 512, 2); else FI_JOIN_LAUNCH(2, 1024, 1);
+  } else {
+    if (two) FI_JOIN_LAUNCH(0, 512, 2); else FI_JOIN_LAUNCH(0, 1024, 1);
+  }
+#undef FI_JOIN_LAUNCH
   return cudaGetLastError();
 }
 

@@ -83,8 +83,8 @@ uint32_t hierarchical_hi_bits(uint32_t radix_bits);
 // ---- radix join ---------------------------------------------------------
 struct JoinScratch {
   uint32_t *item_start;   // [fanout + 1]
-  uint32_t *item_counter; // [1]
-  uint64_t *tile_state;   // look-back state for the item scan
+  uint32_t *item_part;    // [join_items_capacity(fanout, probe_len)]
+  uint64_t *tile_state;   // [fanout / 1024 + 2] look-back state of the plan
   uint32_t *tile_counter; // [1]
   int *status;
 };
@@ -109,7 +109,7 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
                               int64_t *result_set, uint64_t *match_count,
                               JoinScratch s, uint32_t sm_count,
                               cudaStream_t stream);
-uint32_t join_items_capacity(uint32_t fanout);
+uint32_t join_items_capacity(uint32_t fanout, uint64_t probe_len);
 
 // ---- no-partitioning join ------------------------------------------------
 template <typename K>

@@ -310,8 +310,8 @@ class GpuRadixPartitioner:
             C.c_uint64(dmem_buffer_bytes), C.byref(self.h)))
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().fi_gpu_radix_partitioner_free(self.h)
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_gpu_radix_partitioner_free(self.h)
             self.h = None
 
     def status(self):
@@ -380,8 +380,8 @@ class CudaRadixJoin:
             C.c_uint32(grid_size), C.c_uint32(block_size), C.byref(self.h)))
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().fi_cuda_radix_join_free(self.h)
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_cuda_radix_join_free(self.h)
             self.h = None
 
     def status(self):
@@ -426,8 +426,8 @@ class CudaHashJoin:
             C.c_uint32(probe_dim[1]), C.byref(self.h)))
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().fi_cuda_hash_join_free(self.h)
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_cuda_hash_join_free(self.h)
             self.h = None
 
     def build(self, join_attr, payload_attr, stream=None):
@@ -459,8 +459,8 @@ class RadixJoinEngine:
         self.result = torch.zeros(2, dtype=torch.int64, device="cuda")
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().fi_radix_join_engine_free(self.h)
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_radix_join_engine_free(self.h)
             self.h = None
 
     def workspace_bytes(self):
