@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "tile_scatter.cuh"
+#include "tma_scatter.cuh"
 
 namespace fi {
 
@@ -214,6 +215,64 @@ __global__ void __launch_bounds__(Pass2Shape<K>::kThreads, Pass2Shape<K>::kMinBl
   RegionSource<K> src(rel1, reg_pre, reg_begin, C1);
   tile_scatter_range<K, Pass2Shape<K>>(src, s0, s1, F2, mask2, ign2, cur, toff, scan_tmp,
                         staged, rel2, base, rel2_len, status);
+}
+
+// The same scatter fed by TMA bulk copies of the region segments (16-byte
+// tuples only).  Shared memory: bars | reg_pre | reg_begin | stages |
+// staged tile | toff | cur | scan_tmp.
+__host__ __device__ inline size_t pass2_tma_tables_bytes(uint32_t C1) {
+  return (64 + (2 * (size_t)C1 + 1) * 8 + 127) & ~(size_t)127;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
+    pass2_scatter_tma_kernel(const Tuple<K> *__restrict__ rel1,
+                             const uint64_t *__restrict__ off1, uint32_t C1,
+                             uint32_t F1, uint32_t F2, uint64_t mask2,
+                             uint32_t ign2, Pass2Plan pl,
+                             Tuple<K> *__restrict__ rel2, uint64_t rel2_len,
+                             int *status) {
+  using S = TmaShape<K>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  uint64_t *reg_pre = bars + 8;             // [C1 + 1]
+  uint64_t *reg_begin = reg_pre + C1 + 1;   // [C1]
+  unsigned char *stages = smem_raw + pass2_tma_tables_bytes(C1);
+  Tuple<K> *staged =
+      reinterpret_cast<Tuple<K> *>(stages + S::kStages * tma_stage_bytes<K>());
+  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + S::kTile);
+  uint32_t *cur = toff + F2 + 1;
+  uint32_t *scan_tmp = cur + F2;
+  const uint32_t k = blockIdx.x;
+  const uint32_t total = pl.piece_first[F1];
+  if (k >= total) return;
+  const uint32_t p1 = find_p1(pl.piece_first, F1, k);
+  const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
+  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  const uint64_t *cp = pl.cursor + (uint64_t)k * F2;
+  const uint64_t base = cp[0];
+  for (uint32_t p = threadIdx.x; p < F2; p += blockDim.x)
+    cur[p] = (uint32_t)(cp[p] - base);
+  for (uint32_t p = threadIdx.x; p <= F2; p += blockDim.x) toff[p] = 0;
+  const uint64_t *rp = pl.reg_pre + (uint64_t)p1 * (C1 + 1);
+  for (uint32_t c = threadIdx.x; c <= C1; c += blockDim.x) {
+    reg_pre[c] = rp[c];
+    if (c < C1) reg_begin[c] = off1[(uint64_t)c * F1 + p1];
+  }
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < S::kStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  TmaRegionSource<K> src(rel1, reg_pre, reg_begin, C1);
+  tma_tile_scatter_range<K>(src, s0, s1, F2, mask2, ign2, cur, toff, scan_tmp,
+                            staged, stages, bars, rel2, base, rel2_len, status);
+}
+
+template <typename K>
+size_t pass2_tma_smem(uint32_t C1, uint32_t F2) {
+  return pass2_tma_tables_bytes(C1) + tma_scatter_smem<K>(F2) - 64;
 }
 
 template <typename K>
@@ -477,15 +536,35 @@ static int engine_run(fi_radix_join_engine *e, const K *bk, const K *bp,
       pass2_cursor_kernel<<<F1, 1024, csm, st>>>(F1, F2, pl);
       FI_CK(cudaGetLastError(), "pass-2 cursors");
       e->mark(3 + 4 * r, st);
-      const size_t ssm = pass2_scatter_smem<K>(C1, F2);
-      FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_kernel<K>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ssm),
-            "smem attribute");
-      pass2_scatter_kernel<K><<<e->max_pieces, Pass2Shape<K>::kThreads, ssm, st>>>(
-          (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
-          C1, F1, F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, lens[r],
-          (int *)e->status.ptr);
+      bool tma_done = false;
+      if constexpr (sizeof(Tuple<K>) == 16) {
+        // TMA-fed stages (the pass-1 relation is a 16-byte aligned
+        // allocation of 16-byte tuples, so every region segment qualifies)
+        const size_t tsm = pass2_tma_smem<K>(C1, F2);
+        if (tsm <= (size_t)device_max_smem_optin()) {
+          FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_tma_kernel<K>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tsm),
+                "smem attribute");
+          pass2_scatter_tma_kernel<K>
+              <<<e->max_pieces, TmaShape<K>::kThreads, tsm, st>>>(
+                  (const Tuple<K> *)e->rel1[r].ptr,
+                  (const uint64_t *)e->off1[r].ptr, C1, F1, F2, mask2, b1, pl,
+                  (Tuple<K> *)e->rel2[r].ptr, lens[r], (int *)e->status.ptr);
+          tma_done = true;
+        }
+      }
+      if (!tma_done) {
+        const size_t ssm = pass2_scatter_smem<K>(C1, F2);
+        FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_kernel<K>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)ssm),
+              "smem attribute");
+        pass2_scatter_kernel<K><<<e->max_pieces, Pass2Shape<K>::kThreads, ssm, st>>>(
+            (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
+            C1, F1, F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, lens[r],
+            (int *)e->status.ptr);
+      }
       FI_CK(cudaGetLastError(), "pass-2 scatter");
       e->mark(4 + 4 * r, st);
       e->launches += hist_launches + 1 + 4;

@@ -9,10 +9,12 @@
 // B200 design of the write-combining scatter ("tile scatter",
 // tile_scatter.cuh):
 //  * One CTA owns one chunk (the Chunked layout's unit) and walks it in tiles.
-//    The next tile's keys and payloads are loaded into registers
-//    (evict-first) while the current tile is processed, so HBM reads stay in
-//    flight across the block barriers.  With at least two chunks per SM the
-//    CTAs are 256 threads wide and two share an SM.
+//    The next tile's keys and payloads are brought into a shared-memory
+//    stage by TMA bulk copies (tma_scatter.cuh) while the current tile is
+//    processed, so HBM reads stay in flight across the block barriers and
+//    the CTA can run 1024 threads.  Columns that are not 16-byte aligned, or
+//    fanouts whose stages do not fit shared memory, use the same algorithm
+//    with a register double buffer (tile_scatter.cuh).
 //  * Each tile is counting-sorted by partition in shared memory (shared
 //    atomic ranks + a block scan of the tile histogram) into a staging
 //    buffer, then written out in partition runs: consecutive threads write
@@ -26,6 +28,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "tile_scatter.cuh"
+#include "tma_scatter.cuh"
 
 namespace fi {
 
@@ -58,6 +61,46 @@ __global__ void __launch_bounds__(S::kThreads, S::kMinBlocks)
   ColumnSource<K> src{keys, pays};
   tile_scatter_range<K, S>(src, cb, ce, F, mask, ignore_bits, cur, toff,
                            scan_tmp, staged, out, base, out_len, status);
+}
+
+// Same as tile_scatter_kernel with TMA-fed input stages (tma_scatter.cuh).
+// Shared memory: bars | stages | staged tile | toff | cur | scan_tmp.
+template <typename K>
+__global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
+    tma_tile_scatter_kernel(const K *__restrict__ keys,
+                            const K *__restrict__ pays, uint64_t len,
+                            uint64_t clen, uint32_t chunks, uint32_t radix_bits,
+                            uint32_t ignore_bits,
+                            const uint64_t *__restrict__ cursors,
+                            Tuple<K> *__restrict__ out, uint64_t out_len,
+                            int *status) {
+  using S = TmaShape<K>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *stages = smem_raw + 64;
+  Tuple<K> *staged =
+      reinterpret_cast<Tuple<K> *>(stages + S::kStages * tma_stage_bytes<K>());
+  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + S::kTile);
+  uint32_t *cur = toff + F + 1;
+  uint32_t *scan_tmp = cur + F;
+
+  const uint32_t c = blockIdx.x;
+  const uint64_t cb = clen * c, ce = (c + 1 == chunks) ? len : cb + clen;
+  const uint64_t base = cursors[(uint64_t)c * F];
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    cur[p] = (uint32_t)(cursors[(uint64_t)c * F + p] - base);
+  for (uint32_t p = threadIdx.x; p <= F; p += blockDim.x) toff[p] = 0;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < S::kStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  TmaColumnSource<K> src{keys, pays};
+  tma_tile_scatter_range<K>(src, cb, ce, F, mask, ignore_bits, cur, toff,
+                            scan_tmp, staged, stages, bars, out, base, out_len,
+                            status);
 }
 
 // Non-caching scatter: one shared-memory atomic per tuple and a direct
@@ -157,6 +200,20 @@ static cudaError_t launch_tile(const K *keys, const K *pays, uint64_t len,
                                cudaStream_t stream) {
   constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
   const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
+  // TMA-fed stages when both columns are 16-byte aligned and the stages fit
+  const size_t tma_sm = tma_scatter_smem<K>(1u << radix_bits);
+  if ((reinterpret_cast<uintptr_t>(keys) % 16) == 0 &&
+      (reinterpret_cast<uintptr_t>(pays) % 16) == 0 &&
+      tma_sm <= (size_t)device_max_smem_optin()) {
+    cudaError_t e = cudaFuncSetAttribute(
+        (const void *)tma_tile_scatter_kernel<K>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_sm);
+    if (e != cudaSuccess) return e;
+    tma_tile_scatter_kernel<K><<<chunks, TmaShape<K>::kThreads, tma_sm, stream>>>(
+        keys, pays, len, clen, chunks, radix_bits, ignore_bits, cursors,
+        reinterpret_cast<Tuple<K> *>(out), out_len, status);
+    return cudaGetLastError();
+  }
   return launch_tile_shape<K, TileWide<K>>(keys, pays, len, clen, chunks,
                                            radix_bits, ignore_bits, cursors,
                                            out, out_len, status, stream);

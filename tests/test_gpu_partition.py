@@ -126,6 +126,33 @@ def test_partition(fi, oracle, ndt, tdt, algo, hist, n, grid, bits):
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("bits", [5, 11, 13])
+def test_partition_unaligned_columns(fi, oracle, ndt, tdt, bits):
+    """Columns that start off a 16-byte boundary take the register-fed scatter
+    instead of the TMA-fed one; the result must be the same."""
+    n, grid = 300001, 20
+    keys, pays = gen(oracle, n, ndt, 12)
+    dk = torch.empty(n + 1, dtype=tdt, device="cuda")[1:]
+    dp = torch.empty(n + 1, dtype=tdt, device="cuda")[1:]
+    dk.copy_(to_dev(keys))
+    dp.copy_(to_dev(pays))
+    p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Chunked,
+                               fi.GpuRadixPartitionAlgorithm.SSWWCv2,
+                               fi.RadixBits(bits), grid, 1024)
+    o = fi.PartitionOffsets(fi.GpuHistogramAlgorithm.Chunked, grid, bits, tdt)
+    rel = fi.PartitionedRelation(n, fi.GpuHistogramAlgorithm.Chunked, bits, grid, tdt,
+                                 fill=-1)
+    p.prefix_sum(fi.RadixPass.First, dk, o)
+    p.partition(fi.RadixPass.First, dk, dp, o, rel)
+    p.status()
+    off = oracle.chunked_prefix_sum(keys, grid, bits)
+    padded = rel.padded_len()
+    ref = oracle.chunked_radix_partition(keys, pays, off, grid, bits, 0, padded)
+    assert_same_partitions(to_host(rel.relation)[:padded], ref, off, grid, bits,
+                           padded, oracle.padding_len(ndt))
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
 @pytest.mark.parametrize("bits", [15])
 def test_partition_hierarchical(fi, oracle, ndt, tdt, bits):
     """Fanouts above the single-level tile scatter use the two-level scatter."""
