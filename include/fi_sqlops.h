@@ -251,6 +251,27 @@ int fi_gpu_partition_int64(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
                            fi_partition_offsets *offsets,
                            fi_partitioned_relation *rel, fi_stream_t stream);
 
+/* Chunked prefix sum that allocates no device memory.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc (an engine that
+ * owns all device memory through its own pool, a host that forbids
+ * allocation on its threads, code that must not stall a stream on an
+ * allocation): same offsets as fi_gpu_prefix_sum_int64 on a Chunked
+ * partitioner with grid = num_chunks, pass bits = radix_bits and
+ * ignore_bits, but the scratch counters live in a fixed 2 MiB array inside
+ * the library (held on every GPU that loads it until exit).  Limit:
+ * num_chunks * 2^radix_bits <= 524288 counters, radix_bits <= 15; larger
+ * requests fail with FI_ERR_INVALID_ARGUMENT.  The caller passes the keys
+ * and the offsets buffer (num_chunks * 2^radix_bits u64).  All calls share
+ * the array: calls that overlap on the GPU race; serialise them.  The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress), so
+ * make it before capturing the stream into a graph. */
+int fi_gpu_chunked_prefix_sum_noalloc_int64(const int64_t *partition_attr,
+                                            uint64_t len, uint32_t num_chunks,
+                                            uint32_t radix_bits,
+                                            uint32_t ignore_bits,
+                                            uint64_t *offsets,
+                                            fi_stream_t stream);
+
 /* ---- CudaRadixJoin (sql-ops/src/join/cuda_radix_join.rs:116-164) ------ */
 typedef struct fi_cuda_radix_join fi_cuda_radix_join;
 
