@@ -54,6 +54,13 @@ def parse():
                     help="CPU baseline sample: |R| = |S| = 2^cpu_log2n")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--workload", default="join",
+                    choices=["join", "partition"],
+                    help="partition: the partition-only sweep")
+    ap.add_argument("--sweep", default="6,8,10,12,14,16,18",
+                    help="radix bits of the partition sweep")
+    ap.add_argument("--part-log2n", type=int, default=29,
+                    help="partition sweep: 2^part_log2n int64 tuples")
     return ap.parse_args()
 
 
@@ -199,11 +206,12 @@ def cpu_baseline(a, fi, torch):
         r = O.primary_keys(n, a.seed, np.int64)
         s = O.zipf_foreign_keys(n, n, a.zipf, a.seed + 1, a.seed, np.int64)
     threads = os.cpu_count() or 1
+    rp, sp = r.copy(), s.copy()  # payload = key, separate columns
     times = []
     res = None
     for _ in range(2):
         t0 = time.perf_counter()
-        res = O.cpu_radix_join(r, r, s, s, b1, b2, threads, use_reference=True)
+        res = O.cpu_radix_join(r, rp, s, sp, b1, b2, threads, use_reference=True)
         times.append(time.perf_counter() - t0)
     sm, cnt, phases, kind = res
     assert cnt == n, "CPU baseline lost matches"
@@ -243,13 +251,14 @@ def run_reference(a):
         r = O.primary_keys(n, a.seed, np.int64)
         s = O.zipf_foreign_keys(n, n, a.zipf, a.seed + 1, a.seed, np.int64)
     threads = os.cpu_count() or 1
+    rp, sp = r.copy(), s.copy()  # payload = key, separate columns
     kind = None
     for _ in range(a.warmup):
-        O.cpu_radix_join(r, r, s, s, b1, b2, threads, use_reference=True)
+        O.cpu_radix_join(r, rp, s, sp, b1, b2, threads, use_reference=True)
     times = []
     for _ in range(a.steps):
         t0 = time.perf_counter()
-        sm, cnt, _, kind = O.cpu_radix_join(r, r, s, s, b1, b2, threads,
+        sm, cnt, _, kind = O.cpu_radix_join(r, rp, s, sp, b1, b2, threads,
                                             use_reference=True)
         times.append(time.perf_counter() - t0)
     assert cnt == n
@@ -293,6 +302,8 @@ def run_ours(a):
         fi.HashingScheme.Perfect
     seed = a.seed + 1000 * rank
     rk, sk = gen_relations(fi, torch, n, a.zipf, seed)
+    # payload = key, in separate columns (separate memory, as in a table)
+    rp, sp = rk.clone(), sk.clone()
     expected_sum = int(sk.sum().item())
     engine = fi.RadixJoinEngine(n, n, torch.int64, rb, scheme)
     stream = torch.cuda.current_stream()
@@ -301,7 +312,7 @@ def run_ours(a):
     # foreign key, so count = |S| and sum = sum(S.payload)
     verified = True
     for _ in range(max(a.warmup, 1)):
-        s, c = engine.run(rk, rk, sk, sk)
+        s, c = engine.run(rk, rp, sk, sp)
         verified = verified and (c == n and s == expected_sum)
     engine.status()
 
@@ -321,7 +332,7 @@ def run_ours(a):
         start.record(stream)
         for k in range(K):
             engine.set_events(ev_sets[k])
-            engine.run_async(rk, rk, sk, sk)
+            engine.run_async(rk, rp, sk, sp)
         end.record(stream)
         torch.cuda.synchronize()
         barrier(world)
@@ -364,20 +375,19 @@ def run_ours(a):
     # e2e through the host-buffer entry point
     e2e = None
     if not a.no_e2e and a.e2e_steps > 0:
-        hk = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        hs = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        hk.copy_(rk)
-        hs.copy_(sk)
-        del rk, sk
+        host = [torch.empty(n, dtype=torch.int64, pin_memory=True) for _ in range(4)]
+        for h, d in zip(host, (rk, rp, sk, sp)):
+            h.copy_(d)
+        del rk, rp, sk, sp
         torch.cuda.empty_cache()
-        engine.run_host(hk, hk, hs, hs)  # warm-up (allocates device columns)
+        engine.run_host(*host)  # warm-up (allocates device columns)
         t_e2e = []
         for _ in range(a.e2e_steps):
             barrier(world)
             t0 = torch.cuda.Event(enable_timing=True)
             t1 = torch.cuda.Event(enable_timing=True)
             t0.record(stream)
-            s, c = engine.run_host(hk, hk, hs, hs)
+            s, c = engine.run_host(*host)
             t1.record(stream)
             torch.cuda.synchronize()
             verified = verified and c == n and s == expected_sum
@@ -387,7 +397,7 @@ def run_ours(a):
                "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 16,
                "ms_per_step": e2e_ms,
                "path": "fi_radix_join_engine_run_host_int64 (pinned host columns)"}
-        del hk, hs
+        del host
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -417,10 +427,137 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def verify_partitioned(torch, keys, pays, rel, chunks, bits, pad):
+    """Size-independent check of one partitioned relation against its input:
+    the offsets equal the chunked prefix sum of the keys, every stored key
+    lies in its region's partition, and per (chunk, partition) region the
+    count and the wrapping sums of keys and payloads equal the input's."""
+    n = keys.numel()
+    F = 1 << bits
+    mask = F - 1
+    clen = ((n + chunks - 1) // chunks) & ~(128 // 8 - 1)
+    idx = torch.arange(n, device="cuda", dtype=torch.int64)
+    chunk = torch.clamp(idx // max(clen, 1), max=chunks - 1)
+    del idx
+    region_in = chunk * F + (keys & mask)
+    del chunk
+    counts = torch.bincount(region_in, minlength=chunks * F)
+    lens = counts.view(chunks, F)
+    excl = torch.cumsum(lens, dim=1) - lens
+    pidx = torch.arange(F, device="cuda", dtype=torch.int64)
+    cidx = torch.arange(chunks, device="cuda", dtype=torch.int64).view(-1, 1)
+    exp_off = excl + (clen + pad * F) * cidx + (pidx + 1) * pad
+    ok = bool(torch.equal(rel.offsets.view(chunks, F), exp_off))
+    ksum = torch.zeros(chunks * F, dtype=torch.int64, device="cuda")
+    psum = torch.zeros_like(ksum)
+    ksum.index_add_(0, region_in, keys)
+    psum.index_add_(0, region_in, pays)
+    del region_in
+    off = rel.offsets.view(-1)
+    slot_region = torch.repeat_interleave(
+        torch.arange(chunks * F, device="cuda", dtype=torch.int64), counts)
+    slot = torch.repeat_interleave(off - torch.cumsum(counts, 0) + counts, counts) + \
+        torch.arange(n, device="cuda", dtype=torch.int64)
+    t = rel.relation.view(-1, 2)
+    gk, gp = t[slot, 0], t[slot, 1]
+    del slot
+    ok = ok and bool(((gk & mask) == (slot_region % F)).all())
+    gks = torch.zeros_like(ksum)
+    gps = torch.zeros_like(psum)
+    gks.index_add_(0, slot_region, gk)
+    gps.index_add_(0, slot_region, gp)
+    return ok and bool(torch.equal(gks, ksum)) and bool(torch.equal(gps, psum))
+
+
+def run_partition_sweep(a):
+    """Partition-only sweep: 2^part_log2n (int64 key, int64 payload) tuples,
+    keys and payloads uniform 64-bit from a seed; one step = Chunked prefix
+    sum + partition over SM-count chunks.  GB/s counts 40 B per tuple (key
+    read + tuple read + tuple write)."""
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    n = 1 << a.part_log2n
+    seed = a.seed + 1000 * rank
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    pays = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_uniform_u64_keys(keys, seed)
+    fi.gen_uniform_u64_keys(pays, seed + 1)
+    chunks = torch.cuda.get_device_properties(0).multi_processor_count
+    peak, peak_kind = load_peaks()
+    stream = torch.cuda.current_stream()
+    pad = fi.padding_len(torch.int64)
+    sweep = []
+    K = a.steps
+    with ClockSampler(local) as clk:
+        for bits in [int(b) for b in a.sweep.split(",")]:
+            # the reference's first-pass choice; the library uses one level
+            # up to 11 bits and two levels above
+            p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Chunked,
+                                       fi.GpuRadixPartitionAlgorithm.HSSWWCv4,
+                                       fi.RadixBits(bits), chunks, 1024)
+            o = fi.PartitionOffsets(fi.GpuHistogramAlgorithm.Chunked, chunks, bits,
+                                    torch.int64)
+            rel = fi.PartitionedRelation(n, fi.GpuHistogramAlgorithm.Chunked, bits,
+                                         chunks, torch.int64)
+            for _ in range(max(a.warmup, 1)):
+                p.prefix_sum(fi.RadixPass.First, keys, o)
+                p.partition(fi.RadixPass.First, keys, pays, o, rel)
+            p.status()
+            evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                   for _ in range(K)]
+            barrier(world)
+            torch.cuda.synchronize()
+            for k in range(K):
+                evs[k][0].record(stream)
+                p.prefix_sum(fi.RadixPass.First, keys, o)
+                evs[k][1].record(stream)
+                p.partition(fi.RadixPass.First, keys, pays, o, rel)
+                evs[k][2].record(stream)
+            torch.cuda.synchronize()
+            barrier(world)
+            p.status()
+            hist_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+            part_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+            step_ms = max_over_ranks(hist_ms + part_ms, world)
+            ok = verify_partitioned(torch, keys, pays, rel, chunks, bits, pad)
+            gbs = world * n * 40 / (step_ms / 1e3) / 1e9
+            sweep.append({"radix_bits": bits, "scatter_levels": 1 if bits <= 11 else 2,
+                          "ms_per_step": step_ms, "prefix_sum_ms": hist_ms,
+                          "partition_ms": part_ms, "gb_per_s": gbs,
+                          "frac": gbs / world / peak,
+                          "prefix_sum_gb_per_s": n * 8 / (hist_ms / 1e3) / 1e9,
+                          "verified": ok})
+            del p, o, rel
+            torch.cuda.empty_cache()
+    clocks = clk.summary()
+    if rank == 0:
+        line = {"metric": "radix partition GB/s",
+                "value": min(r["gb_per_s"] for r in sweep), "unit": "GB/s",
+                "value_is": "the slowest radix-bit setting of the sweep",
+                "n_gpus": world, "steps": K, "warmup": a.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int64",
+                "data": "synthetic (uniform 64-bit keys and payloads from a seed)",
+                "config": {"workload": "radix_partition_%dM_int64_uniform_u64"
+                                       % (n >> 20), "tuples": n, "chunks": chunks,
+                           "histogram": "Chunked",
+                           "l2_flush": "none: inputs (%d GB) larger than L2"
+                                       % (n * 16 // 10**9)},
+                "peak": peak, "peak_source": peak_kind, "sweep": sweep,
+                "clocks": clocks, "verified": all(r["verified"] for r in sweep)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "partition":
+        run_partition_sweep(a)
     else:
         run_ours(a)
 

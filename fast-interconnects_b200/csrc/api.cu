@@ -369,8 +369,8 @@ static int prefix_sum_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
   else
     e = launch_contiguous_prefix_sum<K>(keys, nullptr, len, p->grid, bits,
                                         ignore, pad, nullptr, nullptr,
-                                        o->offsets, o->local_offsets, p->hs(),
-                                        device_sm_count(), stream);
+                                        o->offsets, o->local_offsets, 0,
+                                        p->hs(), device_sm_count(), stream);
   if (e != cudaSuccess) return cuda_error(e, "prefix sum launch");
   return FI_OK;
 }
@@ -434,7 +434,7 @@ static int copy_with_payload_impl(fi_gpu_radix_partitioner *p,
   if (rc) return rc;
   cudaError_t e = launch_contiguous_prefix_sum<K>(
       src_key, src_pay, len, p->grid, bits, ignore, padding_len(2 * sizeof(K)),
-      dst_key, dst_pay, o->offsets, o->local_offsets, p->hs(),
+      dst_key, dst_pay, o->offsets, o->local_offsets, 0, p->hs(),
       device_sm_count(), stream);
   if (e != cudaSuccess) return cuda_error(e, "prefix sum launch");
   return FI_OK;
@@ -522,13 +522,22 @@ extern "C" int fi_gpu_prefix_sum_and_transform_int64(
                                  dst_len, offsets, (cudaStream_t)stream);
 }
 
+// Whether a pass of `bits` uses the hierarchical two-level scatter: above
+// kSingleLevelBits for the write-combining algorithms, and above the
+// single-level limit for all (NC keeps one level while its per-partition
+// counters fit shared memory).
+static bool two_level(const fi_gpu_radix_partitioner *p, uint32_t bits) {
+  return bits > kMaxTileBits ||
+         (bits > kSingleLevelBits && p->algo != FI_PARTITION_NC);
+}
+
 template <typename K>
 static int preallocate_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass) {
   if (!p) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
   uint32_t bits, ignore;
   int rc = p->pass_bits(pass, &bits, &ignore);
   if (rc) return rc;
-  if (bits > kMaxTileBits) {
+  if (two_level(p, bits)) {
     const uint32_t hi = hierarchical_hi_bits(bits);
     rc = p->tmp_cursors.reserve(((size_t)p->grid << hi) * sizeof(uint64_t), false);
     if (rc) return rc;
@@ -603,7 +612,7 @@ static int partition_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
   rc = p->scratch(std::min(F, 1u << kMaxHistBits), chunks);
   if (rc) return rc;
   cudaError_t e;
-  if (bits > kMaxTileBits) {
+  if (two_level(p, bits)) {
     const uint32_t hi = hierarchical_hi_bits(bits);
     rc = p->tmp_cursors.reserve(((size_t)chunks << hi) * sizeof(uint64_t), false);
     if (rc) return rc;

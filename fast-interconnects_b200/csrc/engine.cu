@@ -485,8 +485,8 @@ static int engine_run(fi_radix_join_engine *e, const K *bk, const K *bp,
       padded[r] = lens[r] + (uint64_t)F1 * pad;
       FI_CK(launch_contiguous_prefix_sum<K>(
                 keys[r], nullptr, lens[r], C1, b1, 0, pad, nullptr, nullptr,
-                (uint64_t *)e->off1[r].ptr, (uint64_t *)e->loc1[r].ptr, e->hs(),
-                e->sm_count, st),
+                (uint64_t *)e->off1[r].ptr, (uint64_t *)e->loc1[r].ptr, 0,
+                e->hs(), e->sm_count, st),
             "prefix sum");
       e->mark(1 + 4 * r, st);
       FI_CK(launch_partition<K>(keys[r], pays[r], lens[r], C1, b1, 0,

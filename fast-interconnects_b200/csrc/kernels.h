@@ -33,7 +33,9 @@ cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
                                       uint32_t sm_count, cudaStream_t stream);
 
 // Contiguous prefix sum (radix_partition.cu:105-199 semantics) over the
-// canonical chunks of `grid` blocks: offsets[p] and local_offsets[b*F+p].
+// canonical chunks of `grid` blocks: offsets[p] and local_offsets[b*F+p],
+// both shifted by `base` slots (0 for the reference's semantics; the
+// streamed pass 1 places each block of the input at its own base).
 // When dst_key/dst_pay are given the columns are also copied
 // (prefix_sum_and_copy_with_payload, radix_partition.cu:207-315).
 template <typename K>
@@ -44,7 +46,8 @@ cudaError_t launch_contiguous_prefix_sum(const K *keys, const K *pays,
                                          K *dst_key, K *dst_pay,
                                          uint64_t *offsets,
                                          uint64_t *local_offsets,
-                                         HistScratch s, uint32_t sm_count,
+                                         uint64_t base, HistScratch s,
+                                         uint32_t sm_count,
                                          cudaStream_t stream);
 
 // prefix_sum_and_transform (radix_partition.cu:323-467 semantics).

@@ -9,11 +9,14 @@
 //  * Histogram: every chunk is shared by `splits` CTAs so that the grid fills
 //    all 148 SMs even with few chunks.  Keys stream in with 16-byte
 //    evict-first vector loads; counts go to a shared-memory histogram through
-//    warp-aggregated atomics (match.any), which keeps Zipf-skewed keys from
-//    serialising on one counter.  A chunk owned by a single CTA is scanned in
-//    place and its offsets written directly (one launch); otherwise the CTAs
-//    add their counts into a global per-chunk histogram and a second kernel
-//    scans it.
+//    plain shared atomics (the match.any aggregation of common.cuh measured
+//    slower on B200, even for Zipf-skewed keys).  Fanouts above 2^15 do not
+//    fit one CTA's shared memory: the bins are split into ranges of 2^15 and
+//    every (chunk, split) is read by one CTA per range, the CTAs adjacent in
+//    the grid so the repeated reads come from L2.  A chunk owned by a single
+//    CTA is scanned in place and its offsets written directly (one launch);
+//    otherwise the CTAs add their counts into a global per-chunk histogram
+//    and a second kernel scans it.
 //  * Contiguous offsets: instead of the reference's cooperative launch with
 //    three grid-wide barriers, a second kernel scans the (partition, chunk)
 //    counts with a single-pass decoupled look-back over tiles of partitions
@@ -112,36 +115,49 @@ __device__ __forceinline__ void split_range(uint64_t len, uint64_t clen,
   se = min(ce, sb + per);
 }
 
-// Histogram of one chunk split.  direct_offsets != nullptr: the CTA owns the
-// whole chunk (splits == 1) and writes the chunk's final offsets
-// (radix_partition.cu:83-95); otherwise it adds its counts to g_hist[c*F+p].
-// With dst_key/dst_pay the columns are copied as well.
+// Shared-memory counters of one histogram CTA; larger fanouts are split into
+// ranges of this many bins, one CTA per (chunk, split, range).  The CTAs of
+// one chunk are adjacent in the grid, so their repeated reads of the same
+// keys hit in L2.
+constexpr uint32_t kHistSmemBinsLog2 = 15;
+
+// Histogram of one chunk split, restricted to the bins
+// [range*nbins, (range+1)*nbins), nbins = min(F, 2^15).  direct_offsets !=
+// nullptr: the CTA owns the whole chunk and all bins (splits == ranges == 1)
+// and writes the chunk's final offsets (radix_partition.cu:83-95); otherwise
+// it adds its counts to g_hist[c*F+p].  With dst_key/dst_pay the columns are
+// copied as well.
 template <typename K>
 __global__ void __launch_bounds__(kHistThreads)
     histogram_kernel(const K *__restrict__ keys, const K *__restrict__ pays,
                      K *__restrict__ dst_key, K *__restrict__ dst_pay,
                      uint64_t len, uint64_t clen, uint32_t chunks,
-                     uint32_t splits, uint32_t radix_bits,
+                     uint32_t splits, uint32_t ranges, uint32_t radix_bits,
                      uint32_t ignore_bits, uint32_t pad,
                      uint64_t *__restrict__ direct_offsets,
                      uint32_t *__restrict__ g_hist) {
   extern __shared__ uint32_t smem[];
   const uint32_t F = 1u << radix_bits;
+  const uint32_t nbins = F / ranges;
   const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
   uint32_t *cnt = smem;
-  uint32_t *scan_tmp = smem + F;
-  const uint32_t c = blockIdx.x / splits, s = blockIdx.x % splits;
+  uint32_t *scan_tmp = smem + nbins;
+  const uint32_t r = blockIdx.x % ranges;
+  const uint32_t s = (blockIdx.x / ranges) % splits;
+  const uint32_t c = blockIdx.x / (ranges * splits);
+  const uint32_t bin_lo = r * nbins;
   uint64_t sb, se;
   split_range<K>(len, clen, chunks, c, splits, s, sb, se);
 
-  for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cnt[i] = 0;
+  for (uint32_t i = threadIdx.x; i < nbins; i += blockDim.x) cnt[i] = 0;
   __syncthreads();
 
   for_each_key(keys, sb, se, [&](K key, bool act) {
-    warp_aggregated_count(cnt, key_to_partition(key, mask, ignore_bits), act);
+    const uint32_t b = key_to_partition(key, mask, ignore_bits) - bin_lo;
+    warp_aggregated_count(cnt, b, act && b < nbins);
   });
 
-  if (dst_key != nullptr) {
+  if (dst_key != nullptr && r == 0) {
     for (uint64_t i = sb + threadIdx.x; i < se; i += blockDim.x) {
       dst_key[i] = keys[i];
       dst_pay[i] = pays[i];
@@ -156,28 +172,37 @@ __global__ void __launch_bounds__(kHistThreads)
       direct_offsets[(uint64_t)c * F + p] =
           (uint64_t)cnt[p] + chunk_base + (uint64_t)(p + 1) * pad;
   } else {
-    for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
-      if (cnt[p] != 0) atomicAdd(&g_hist[(uint64_t)c * F + p], cnt[p]);
+    uint32_t *gh = g_hist + (uint64_t)c * F + bin_lo;
+    for (uint32_t p = threadIdx.x; p < nbins; p += blockDim.x)
+      if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
   }
 }
 
-// Per-chunk scan of g_hist into Chunked offsets (one CTA per chunk).
+// Per-chunk scan of g_hist into Chunked offsets (one CTA per chunk), in
+// tiles of kScanTileBins bins with a running carry.
+constexpr uint32_t kScanTileBins = 8192;
 __global__ void __launch_bounds__(1024)
     chunked_scan_kernel(const uint32_t *__restrict__ g_hist, uint32_t F,
                         uint64_t clen, uint32_t pad,
                         uint64_t *__restrict__ offsets) {
   extern __shared__ uint32_t smem[];
+  const uint32_t nb = min(F, kScanTileBins);
   uint32_t *cnt = smem;
-  uint32_t *scan_tmp = smem + F;
+  uint32_t *scan_tmp = smem + nb;
   const uint32_t c = blockIdx.x;
-  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
-    cnt[p] = g_hist[(uint64_t)c * F + p];
-  __syncthreads();
-  block_exclusive_scan_u32(cnt, F, scan_tmp);
   const uint64_t chunk_base = (clen + (uint64_t)pad * F) * c;
-  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
-    offsets[(uint64_t)c * F + p] =
-        (uint64_t)cnt[p] + chunk_base + (uint64_t)(p + 1) * pad;
+  uint64_t carry = 0;
+  for (uint32_t t0 = 0; t0 < F; t0 += nb) {
+    for (uint32_t p = threadIdx.x; p < nb; p += blockDim.x)
+      cnt[p] = g_hist[(uint64_t)c * F + t0 + p];
+    __syncthreads();
+    const uint32_t total = block_exclusive_scan_u32(cnt, nb, scan_tmp);
+    for (uint32_t p = threadIdx.x; p < nb; p += blockDim.x)
+      offsets[(uint64_t)c * F + t0 + p] = carry + (uint64_t)cnt[p] + chunk_base +
+                                          (uint64_t)(t0 + p + 1) * pad;
+    carry += total;
+    __syncthreads();
+  }
 }
 
 // ---- decoupled look-back ---------------------------------------------------
@@ -236,7 +261,7 @@ __device__ uint64_t look_back(uint64_t *tile_state, uint32_t t,
 // kScanTile partitions chained by decoupled look-back.
 __global__ void __launch_bounds__(kScanThreads)
     contiguous_scan_kernel(const uint32_t *__restrict__ g_hist, uint32_t grid,
-                           uint32_t F, uint32_t pad,
+                           uint32_t F, uint32_t pad, uint64_t base,
                            uint64_t *__restrict__ offsets,
                            uint64_t *__restrict__ local_offsets,
                            uint64_t *tile_state, uint32_t *tile_counter,
@@ -257,11 +282,11 @@ __global__ void __launch_bounds__(kScanThreads)
   if (threadIdx.x == 0) prefix_s = look_back(tile_state, t, tile_total, status);
   __syncthreads();
   if (act) {
-    const uint64_t base = prefix_s + excl + (uint64_t)(p + 1) * pad;
-    offsets[p] = base;
+    const uint64_t start = base + prefix_s + excl + (uint64_t)(p + 1) * pad;
+    offsets[p] = start;
     uint64_t run = 0;
     for (uint32_t b = 0; b < grid; ++b) {
-      local_offsets[(uint64_t)b * F + p] = base + run;
+      local_offsets[(uint64_t)b * F + p] = start + run;
       run += g_hist[(uint64_t)b * F + p];
     }
   }
@@ -277,16 +302,17 @@ __global__ void __launch_bounds__(kHistThreads) transform_histogram_kernel(
     uint32_t pid, const Tuple<K> *__restrict__ src,
     const uint64_t *__restrict__ src_offsets, uint32_t src_chunks,
     uint32_t src_fanout, uint64_t src_padded_len, uint32_t src_pad,
-    uint64_t dst_len, uint32_t grid, uint32_t splits, uint32_t radix_bits,
-    uint32_t ignore_bits, K *__restrict__ dst_key, K *__restrict__ dst_pay,
-    uint32_t *__restrict__ g_hist, int *status) {
+    uint64_t dst_len, uint32_t grid, uint32_t splits, uint32_t ranges,
+    uint32_t radix_bits, uint32_t ignore_bits, K *__restrict__ dst_key,
+    K *__restrict__ dst_pay, uint32_t *__restrict__ g_hist, int *status) {
   extern __shared__ uint64_t smem64[];
   const uint32_t F = 1u << radix_bits;
+  const uint32_t nbins = F / ranges;
   const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
   uint64_t *ch_begin = smem64;                 // [src_chunks]
   uint64_t *ch_pre = smem64 + src_chunks;      // [src_chunks + 1]
   uint64_t *tmp64 = ch_pre + src_chunks + 1;   // [33]
-  uint32_t *cnt = reinterpret_cast<uint32_t *>(tmp64 + 33);  // [F]
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(tmp64 + 33);  // [nbins]
 
   // chunk table: begin and length of partition pid in every source chunk
   uint64_t local_len = 0;
@@ -298,7 +324,7 @@ __global__ void __launch_bounds__(kHistThreads) transform_histogram_kernel(
     ch_begin[c] = b;
     ch_pre[c] = e - b;  // length, scanned below
   }
-  for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cnt[i] = 0;
+  for (uint32_t i = threadIdx.x; i < nbins; i += blockDim.x) cnt[i] = 0;
   __syncthreads();
   if (threadIdx.x == 0) {
     uint64_t run = 0;
@@ -318,7 +344,10 @@ __global__ void __launch_bounds__(kHistThreads) transform_histogram_kernel(
   }
   constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
   const uint64_t clen = ((n + grid - 1) / grid) & kAlignMask;
-  const uint32_t b = blockIdx.x / splits, s = blockIdx.x % splits;
+  const uint32_t r = blockIdx.x % ranges;
+  const uint32_t s = (blockIdx.x / ranges) % splits;
+  const uint32_t b = blockIdx.x / (ranges * splits);
+  const uint32_t bin_lo = r * nbins;
   uint64_t sb, se;
   split_range<K>(n, clen, grid, b, splits, s, sb, se);
 
@@ -334,15 +363,19 @@ __global__ void __launch_bounds__(kHistThreads) transform_histogram_kernel(
         if (ch_pre[mid] <= i) lo = mid; else hi = mid;
       }
       Tuple<K> t = load_tuple_cs(src + ch_begin[lo] + (i - ch_pre[lo]));
-      dst_key[i] = t.key;
-      dst_pay[i] = t.value;
+      if (r == 0) {
+        dst_key[i] = t.key;
+        dst_pay[i] = t.value;
+      }
       key = t.key;
     }
-    warp_aggregated_count(cnt, key_to_partition(key, mask, ignore_bits), act);
+    const uint32_t bin = key_to_partition(key, mask, ignore_bits) - bin_lo;
+    warp_aggregated_count(cnt, bin, act && bin < nbins);
   }
   __syncthreads();
-  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
-    if (cnt[p] != 0) atomicAdd(&g_hist[(uint64_t)b * F + p], cnt[p]);
+  uint32_t *gh = g_hist + (uint64_t)b * F + bin_lo;
+  for (uint32_t p = threadIdx.x; p < nbins; p += blockDim.x)
+    if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
 }
 
 // ---- host launchers ---------------------------------------------------------
@@ -353,7 +386,22 @@ uint32_t hist_splits(uint32_t chunks, uint32_t sm_count) {
   return s < 1 ? 1 : s;
 }
 
-static size_t hist_smem(uint32_t F) { return (size_t)(F + 33) * sizeof(uint32_t); }
+// Number of 2^15-bin ranges the histogram of a fanout is split into.
+static uint32_t hist_ranges(uint32_t radix_bits) {
+  return radix_bits > kHistSmemBinsLog2 ? 1u << (radix_bits - kHistSmemBinsLog2)
+                                        : 1u;
+}
+
+// Shared memory of one histogram CTA: its bins plus the scan's warp sums.
+static size_t hist_smem(uint32_t radix_bits) {
+  return (size_t)(((1u << radix_bits) / hist_ranges(radix_bits)) + 33) *
+         sizeof(uint32_t);
+}
+
+static size_t scan_smem(uint32_t F) {
+  return (size_t)((F < kScanTileBins ? F : kScanTileBins) + 33) *
+         sizeof(uint32_t);
+}
 
 template <typename K>
 static cudaError_t set_smem(const void *fn, size_t bytes) {
@@ -371,31 +419,34 @@ cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
   constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
   const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
   const uint32_t splits = hist_splits(chunks, sm_count);
-  const size_t sm = hist_smem(F);
+  const uint32_t ranges = hist_ranges(radix_bits);
+  const size_t sm = hist_smem(radix_bits);
   cudaError_t e = set_smem<K>((const void *)histogram_kernel<K>, sm);
   if (e != cudaSuccess) return e;
-  if (splits == 1) {
+  if (splits == 1 && ranges == 1) {
     histogram_kernel<K><<<chunks, kHistThreads, sm, stream>>>(
-        keys, nullptr, nullptr, nullptr, len, clen, chunks, 1, radix_bits,
+        keys, nullptr, nullptr, nullptr, len, clen, chunks, 1, 1, radix_bits,
         ignore_bits, pad, offsets, nullptr);
     return cudaGetLastError();
   }
   e = cudaMemsetAsync(s.hist, 0, (size_t)chunks * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  histogram_kernel<K><<<chunks * splits, kHistThreads, sm, stream>>>(
-      keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, radix_bits,
-      ignore_bits, pad, nullptr, s.hist);
+  histogram_kernel<K><<<chunks * splits * ranges, kHistThreads, sm, stream>>>(
+      keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, ranges,
+      radix_bits, ignore_bits, pad, nullptr, s.hist);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  e = set_smem<K>((const void *)chunked_scan_kernel, sm);
+  const size_t ssm = scan_smem(F);
+  e = set_smem<K>((const void *)chunked_scan_kernel, ssm);
   if (e != cudaSuccess) return e;
-  chunked_scan_kernel<<<chunks, 1024, sm, stream>>>(s.hist, F, clen, pad,
-                                                    offsets);
+  chunked_scan_kernel<<<chunks, 1024, ssm, stream>>>(s.hist, F, clen, pad,
+                                                     offsets);
   return cudaGetLastError();
 }
 
 static cudaError_t launch_contiguous_scan(uint32_t F, uint32_t grid,
-                                          uint32_t pad, uint64_t *offsets,
+                                          uint32_t pad, uint64_t base,
+                                          uint64_t *offsets,
                                           uint64_t *local_offsets,
                                           HistScratch s, cudaStream_t stream) {
   const uint32_t tiles = (F + kScanTile - 1) / kScanTile;
@@ -405,7 +456,7 @@ static cudaError_t launch_contiguous_scan(uint32_t F, uint32_t grid,
   e = cudaMemsetAsync(s.tile_counter, 0, sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
   contiguous_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(
-      s.hist, grid, F, pad, offsets, local_offsets, s.tile_state,
+      s.hist, grid, F, pad, base, offsets, local_offsets, s.tile_state,
       s.tile_counter, s.status);
   return cudaGetLastError();
 }
@@ -418,23 +469,26 @@ cudaError_t launch_contiguous_prefix_sum(const K *keys, const K *pays,
                                          K *dst_key, K *dst_pay,
                                          uint64_t *offsets,
                                          uint64_t *local_offsets,
-                                         HistScratch s, uint32_t sm_count,
+                                         uint64_t base, HistScratch s,
+                                         uint32_t sm_count,
                                          cudaStream_t stream) {
   const uint32_t F = 1u << radix_bits;
   constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
   const uint64_t clen = ((len + grid - 1) / grid) & kAlignMask;
   const uint32_t splits = hist_splits(grid, sm_count);
-  const size_t sm = hist_smem(F);
+  const uint32_t ranges = hist_ranges(radix_bits);
+  const size_t sm = hist_smem(radix_bits);
   cudaError_t e = set_smem<K>((const void *)histogram_kernel<K>, sm);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(s.hist, 0, (size_t)grid * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
-      keys, pays, dst_key, dst_pay, len, clen, grid, splits, radix_bits,
-      ignore_bits, pad, nullptr, s.hist);
+  histogram_kernel<K><<<grid * splits * ranges, kHistThreads, sm, stream>>>(
+      keys, pays, dst_key, dst_pay, len, clen, grid, splits, ranges,
+      radix_bits, ignore_bits, pad, nullptr, s.hist);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return launch_contiguous_scan(F, grid, pad, offsets, local_offsets, s, stream);
+  return launch_contiguous_scan(F, grid, pad, base, offsets, local_offsets, s,
+                                stream);
 }
 
 template <typename K>
@@ -447,21 +501,24 @@ cudaError_t launch_prefix_sum_and_transform(
     uint32_t sm_count, cudaStream_t stream) {
   const uint32_t F = 1u << radix_bits;
   const uint32_t splits = hist_splits(grid, sm_count);
+  const uint32_t ranges = hist_ranges(radix_bits);
   const size_t sm = (size_t)(2 * src_chunks + 1 + 33) * sizeof(uint64_t) +
-                    (size_t)F * sizeof(uint32_t);
+                    (size_t)(F / ranges) * sizeof(uint32_t);
   cudaError_t e =
       set_smem<K>((const void *)transform_histogram_kernel<K>, sm);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(s.hist, 0, (size_t)grid * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  transform_histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
-      partition_id, reinterpret_cast<const Tuple<K> *>(src_relation),
-      src_offsets, src_chunks, 1u << src_radix_bits, src_padded_len, src_pad,
-      dst_len, grid, splits, radix_bits, ignore_bits, dst_key, dst_pay, s.hist,
-      s.status);
+  transform_histogram_kernel<K>
+      <<<grid * splits * ranges, kHistThreads, sm, stream>>>(
+          partition_id, reinterpret_cast<const Tuple<K> *>(src_relation),
+          src_offsets, src_chunks, 1u << src_radix_bits, src_padded_len,
+          src_pad, dst_len, grid, splits, ranges, radix_bits, ignore_bits,
+          dst_key, dst_pay, s.hist, s.status);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return launch_contiguous_scan(F, grid, pad, offsets, local_offsets, s, stream);
+  return launch_contiguous_scan(F, grid, pad, 0, offsets, local_offsets, s,
+                                stream);
 }
 
 #define FI_INSTANTIATE_PREFIX(K)                                               \
@@ -470,7 +527,8 @@ cudaError_t launch_prefix_sum_and_transform(
       HistScratch, uint32_t, cudaStream_t);                                    \
   template cudaError_t launch_contiguous_prefix_sum<K>(                        \
       const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t, uint32_t,  \
-      K *, K *, uint64_t *, uint64_t *, HistScratch, uint32_t, cudaStream_t);  \
+      K *, K *, uint64_t *, uint64_t *, uint64_t, HistScratch, uint32_t,       \
+      cudaStream_t);                                                           \
   template cudaError_t launch_prefix_sum_and_transform<K>(                     \
       uint32_t, const void *, const uint64_t *, uint32_t, uint32_t, uint64_t,  \
       uint32_t, uint64_t, uint32_t, uint32_t, uint32_t, uint32_t, K *, K *,    \

@@ -66,8 +66,8 @@ typedef enum {
 /* GpuRadixPartitionAlgorithm (gpu_radix_partition.rs:233-293).  All five
  * produce the same partitions; on B200 they select between the per-tuple
  * scatter (NC) and the shared-memory tile write-combining scatter (the
- * others), and HSSWWC_V4 also selects the hierarchical two-level scatter for
- * fanouts above 2^11. */
+ * others), which becomes the hierarchical two-level scatter for fanouts
+ * above 2^11 (NC: above 2^14). */
 typedef enum {
   FI_PARTITION_NC = 0,
   FI_PARTITION_LASWWC = 1,
@@ -259,7 +259,7 @@ int fi_gpu_partition_int64(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
  * partitioner with grid = num_chunks, pass bits = radix_bits and
  * ignore_bits, but the scratch counters live in a fixed 2 MiB array inside
  * the library (held on every GPU that loads it until exit).  Limit:
- * num_chunks * 2^radix_bits <= 524288 counters, radix_bits <= 15; larger
+ * num_chunks * 2^radix_bits <= 524288 counters, radix_bits <= 18; larger
  * requests fail with FI_ERR_INVALID_ARGUMENT.  The caller passes the keys
  * and the offsets buffer (num_chunks * 2^radix_bits u64).  All calls share
  * the array: calls that overlap on the GPU race; serialise them.  The first

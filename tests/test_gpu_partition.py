@@ -30,7 +30,10 @@ def gen(oracle, n, dt, seed, kind="pk"):
 
 CHUNKED_CASES = [(100, 1, 0), (100, 4, 2), (1000, 80, 9), (10**6, 8, 6),
                  (10**6, 10, 10), (1 << 20, 148, 12), (1 << 20, 148, 14),
-                 (1 << 18, 3, 15), (8 * 2**20, 148, 9)]
+                 (1 << 18, 3, 15), (8 * 2**20, 148, 9),
+                 # fanouts above one CTA's shared-memory histogram (bin ranges)
+                 (1000, 3, 17), (1 << 20, 16, 16), (1 << 19, 4, 18),
+                 (1 << 20, 148, 16)]
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
@@ -51,7 +54,8 @@ def test_chunked_prefix_sum(fi, oracle, ndt, tdt, n, grid, bits):
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
 @pytest.mark.parametrize("n,grid,bits", [(100, 1, 0), (1000, 80, 9),
                                          (10**6, 10, 10), (1 << 20, 148, 12),
-                                         (1 << 18, 7, 15)])
+                                         (1 << 18, 7, 15), (1 << 20, 5, 16),
+                                         (1 << 19, 3, 18)])
 def test_contiguous_prefix_sum(fi, oracle, ndt, tdt, n, grid, bits):
     keys, _ = gen(oracle, n, ndt, 2)
     p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Contiguous,
@@ -153,18 +157,31 @@ def test_partition_unaligned_columns(fi, oracle, ndt, tdt, bits):
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
-@pytest.mark.parametrize("bits", [15])
-def test_partition_hierarchical(fi, oracle, ndt, tdt, bits):
-    """Fanouts above the single-level tile scatter use the two-level scatter."""
-    n, grid = 1 << 20, 16
-    keys, pays = gen(oracle, n, ndt, 5)
-    rel = run_partition(fi, oracle, keys, pays, tdt, fi.GpuHistogramAlgorithm.Chunked,
+@pytest.mark.parametrize("hist,bits,grid", [("Chunked", 15, 16), ("Chunked", 16, 16),
+                                            ("Chunked", 17, 5), ("Chunked", 18, 4),
+                                            ("Contiguous", 16, 8),
+                                            ("Contiguous", 18, 3)])
+def test_partition_hierarchical(fi, oracle, ndt, tdt, hist, bits, grid):
+    """Fanouts above the single-level tile scatter (2^15..2^18, the
+    partition sweep's "hierarchical" fanouts) use the two-level scatter."""
+    n = 1 << 20
+    keys, pays = gen(oracle, n, ndt, 5, kind="u64")
+    H = getattr(fi.GpuHistogramAlgorithm, hist)
+    rel = run_partition(fi, oracle, keys, pays, tdt, H,
                         fi.GpuRadixPartitionAlgorithm.HSSWWCv4, grid, bits)
-    off = oracle.chunked_prefix_sum(keys, grid, bits)
+    if hist == "Chunked":
+        off = oracle.chunked_prefix_sum(keys, grid, bits)
+        cursors, chunks = off, grid
+    else:
+        off, cursors = oracle.contiguous_prefix_sum(keys, grid, bits)
+        chunks = 1
+    np.testing.assert_array_equal(to_host(rel.offsets).astype(np.uint64), off)
     padded = rel.padded_len()
-    ref = oracle.chunked_radix_partition(keys, pays, off, grid, bits, 0, padded)
-    assert_same_partitions(to_host(rel.relation)[:padded], ref, off, grid, bits,
-                           padded, oracle.padding_len(ndt))
+    ref = oracle.chunked_radix_partition(keys, pays, cursors, grid, bits, 0, padded)
+    got = to_host(rel.relation)[:padded]
+    assert_same_partitions(got, ref, off, chunks, bits, padded,
+                           oracle.padding_len(ndt))
+    assert (got[:, 0] != -1).sum() == n
 
 
 @pytest.mark.parametrize("algo", ["NC", "SSWWCv2"])
@@ -196,7 +213,7 @@ def test_partition_uniform_64bit_keys(fi, oracle):
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
-@pytest.mark.parametrize("b1,b2", [(0, 0), (2, 2), (6, 6), (10, 10)])
+@pytest.mark.parametrize("b1,b2", [(0, 0), (2, 2), (6, 6), (10, 10), (2, 16)])
 def test_two_pass_transform_and_partition(fi, oracle, ndt, tdt, b1, b2):
     """Reference two-pass flow (test_gpu_radix_partition.rs two_pass_*):
     pass 1 Chunked, then per first-pass partition prefix_sum_and_transform and
