@@ -625,8 +625,9 @@ static int partition_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
   } else {
     e = launch_partition<K>(keys, pays, len, chunks, bits, ignore, cursors,
                             r->relation, r->relation_len,
-                            p->algo == FI_PARTITION_NC, (int *)p->status.ptr,
-                            stream);
+                            p->algo == FI_PARTITION_NC ? kScatterNC
+                                                       : kScatterAuto,
+                            (int *)p->status.ptr, stream);
   }
   if (e != cudaSuccess) return cuda_error(e, "partition launch");
   return FI_OK;

@@ -300,17 +300,32 @@ using namespace fi;
 
 struct fi_radix_join_engine {
   uint64_t max_build, max_probe;
-  uint32_t tuple_bytes;
-  int32_t bits1, bits2;  // bits2 < 0: single pass
+  uint32_t tuple_bytes;   // largest tuple the buffers hold (8 or 16 bytes)
+  int32_t bits1, bits2;   // current plan; bits2 < 0: single pass
+  int32_t cap1, cap2;     // bits the buffers were sized for
   fi_hashing_scheme scheme;
+  uint32_t join_block = kJoinBlock;
+  uint32_t scatter = 0;   // 0: TMA-fed where possible, 1: register-fed
   uint32_t sm_count, C1, F1, F2, max_pieces;
   DevBuf rel1[2], off1[2], loc1[2], rel2[2];
   DevBuf reg_pre[2], p1_base[2], piece_first[2], piece_tmp[2], hist2[2],
       cursor2[2], off2[2];
   DevBuf hist_scratch, tile_state, counters, status;
   DevBuf join_items, join_part, join_counters, join_tiles, join_sums, join_count;
-  uint32_t join_grid() const { return sm_count * kJoinCtasPerSm; }
+  int scatter_variant() const {
+    return scatter == 1 ? kScatterRegisters : kScatterAuto;
+  }
+  uint32_t join_grid() const {
+    return sm_count * (join_block > 512 ? 1u : kJoinCtasPerSm);
+  }
   DevBuf in_cols[4];  // device copies of host input (run_host)
+  uint64_t part_len[2] = {0, 0};  // lengths of the partitioned relations
+  bool built = false;             // a build relation is partitioned
+  // streamed pass 1 (run_streamed): a copy stream, two staging slots of
+  // key and payload columns, their ready/free events, block-local cursors
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t slot_ready[2] = {}, slot_free[2] = {};
+  DevBuf stage_key[2], stage_pay[2], stream_loc, result_dev;
   uint64_t workspace = 0;
   cudaEvent_t events[FI_ENGINE_PHASE_EVENTS] = {};
   bool record = false;
@@ -346,6 +361,17 @@ struct fi_radix_join_engine {
     join_counters.release();
     join_tiles.release(); join_sums.release(); join_count.release();
     for (auto &b : in_cols) b.release();
+    for (int i = 0; i < 2; ++i) {
+      stage_key[i].release();
+      stage_pay[i].release();
+      if (slot_ready[i]) cudaEventDestroy(slot_ready[i]);
+      if (slot_free[i]) cudaEventDestroy(slot_free[i]);
+      slot_ready[i] = slot_free[i] = nullptr;
+    }
+    stream_loc.release();
+    result_dev.release();
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
   }
 };
 
@@ -375,8 +401,8 @@ extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
   e->max_build = max_build_len;
   e->max_probe = max_probe_len;
   e->tuple_bytes = tuple_bytes;
-  e->bits1 = b1;
-  e->bits2 = b2;
+  e->bits1 = e->cap1 = b1;
+  e->bits2 = e->cap2 = b2;
   e->scheme = hashing_scheme;
   e->sm_count = (uint32_t)device_sm_count();
   e->C1 = e->sm_count * kChunksPerSm;
@@ -392,7 +418,7 @@ extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
     rc = e->alloc(e->rel1[r], (lens[r] + (uint64_t)pass1_chunks * e->F1 * pad) *
                                   tuple_bytes);
     if (!rc) rc = e->alloc(e->off1[r], (size_t)e->C1 * e->F1 * 8);
-    if (!rc && b2 < 0) rc = e->alloc(e->loc1[r], (size_t)e->C1 * e->F1 * 8);
+    if (!rc) rc = e->alloc(e->loc1[r], (size_t)e->C1 * e->F1 * 8);
     if (!rc && b2 >= 0) {
       rc = e->alloc(e->rel2[r], std::max<uint64_t>(lens[r], 1) * tuple_bytes);
       if (!rc) rc = e->alloc(e->reg_pre[r], (size_t)e->F1 * (e->C1 + 1) * 8);
@@ -410,13 +436,17 @@ extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
   if (!rc) rc = e->alloc(e->counters, 16, true);
   if (!rc) rc = e->alloc(e->status, 16, true);
   if (!rc) rc = e->alloc(e->join_items, ((size_t)Fj + 1) * 4);
+  // item capacity for the largest padding in tuples (8-byte tuples)
   if (!rc)
     rc = e->alloc(e->join_part,
                   (size_t)join_items_capacity(
-                      Fj, max_probe_len + (uint64_t)e->F1 * pad) * 4);
+                      Fj, max_probe_len + (uint64_t)e->F1 * (kPaddingBytes / 8)) *
+                      4);
   if (!rc) rc = e->alloc(e->join_counters, 16, true);
   if (!rc) rc = e->alloc(e->join_tiles, ((size_t)Fj / 1024 + 2) * 8, true);
-  if (!rc) rc = e->alloc(e->join_sums, (size_t)e->join_grid() * kJoinBlock * 8);
+  // per-thread sums for every join shape (grid x block <= 2 x SM x 512)
+  if (!rc)
+    rc = e->alloc(e->join_sums, (size_t)e->sm_count * kJoinCtasPerSm * 512 * 8);
   if (!rc) rc = e->alloc(e->join_count, 16);
   if (rc) {
     e->release_all();
@@ -449,143 +479,213 @@ extern "C" int fi_radix_join_engine_status(fi_radix_join_engine *e) {
     if (e_ != cudaSuccess) return cuda_error(e_, what);                        \
   } while (0)
 
+// Second pass of relation r: from its pass-1 layout (C1 chunks of F1
+// partitions, padded length padded1) into rel2[r], ordered by (p1, p2) with
+// no padding.  Four launches: plan, piece histograms, cursors, scatter.
 template <typename K>
-static int engine_run(fi_radix_join_engine *e, const K *bk, const K *bp,
-                      uint64_t bn, const K *pk, const K *pp, uint64_t pn,
-                      fi_join_result *result, cudaStream_t st) {
-  if (!e || !result) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
-  if (e->tuple_bytes != 2 * sizeof(K))
-    return set_error(FI_ERR_INVALID_ARGUMENT, "engine built for another tuple type");
-  if (bn > e->max_build || pn > e->max_probe)
-    return set_error(FI_ERR_INVALID_ARGUMENT,
-                     "relation larger than the engine's workspace");
-  const uint32_t C1 = e->C1, F1 = e->F1, F2 = e->F2;
+static int engine_pass2(fi_radix_join_engine *e, int r, uint32_t C1,
+                        uint64_t padded1, uint64_t len, cudaStream_t st) {
+  const uint32_t F1 = e->F1, F2 = e->F2;
   const uint32_t b1 = (uint32_t)e->bits1;
-  const uint32_t pad = kPaddingBytes / e->tuple_bytes;
-  const K *keys[2] = {bk, pk}, *pays[2] = {bp, pp};
-  const uint64_t lens[2] = {bn, pn};
-  const int scheme = e->scheme == FI_HASHING_PERFECT ? 0 : 2;
-  for (int r = 0; r < 2; ++r)
-    if ((uint64_t)(lens[r] + C1 - 1) / C1 >= 0xffffffffull)
-      return set_error(FI_ERR_INTEGER_OVERFLOW, "relation too large");
+  const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
+  const uint64_t mask2 = (uint64_t)(F2 - 1u) << b1;
+  Pass2Plan pl = e->plan(r);
+  pass2_plan_kernel<<<1, 1024, 0, st>>>((const uint64_t *)e->off1[r].ptr, C1, F1,
+                                        padded1, pad, pl,
+                                        (uint64_t *)e->piece_tmp[r].ptr);
+  FI_CK(cudaGetLastError(), "pass-2 plan");
+  piece_histogram_kernel<K><<<e->max_pieces, 512, F2 * 4, st>>>(
+      (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr, C1, F1,
+      F2, mask2, b1, pl);
+  FI_CK(cudaGetLastError(), "pass-2 histogram");
+  const size_t csm = (size_t)(F2 + 33) * 4;
+  pass2_cursor_kernel<<<F1, 1024, csm, st>>>(F1, F2, pl);
+  FI_CK(cudaGetLastError(), "pass-2 cursors");
+  e->mark(3 + 4 * r, st);
+  bool tma_done = false;
+  if constexpr (sizeof(Tuple<K>) == 16) {
+    // TMA-fed stages (the pass-1 relation is a 16-byte aligned allocation of
+    // 16-byte tuples, so every region segment qualifies)
+    const size_t tsm = pass2_tma_smem<K>(C1, F2);
+    if (e->scatter == 0 && tsm <= (size_t)device_max_smem_optin()) {
+      FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_tma_kernel<K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tsm),
+            "smem attribute");
+      pass2_scatter_tma_kernel<K><<<e->max_pieces, TmaShape<K>::kThreads, tsm, st>>>(
+          (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr, C1,
+          F1, F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, len,
+          (int *)e->status.ptr);
+      tma_done = true;
+    }
+  }
+  if (!tma_done) {
+    const size_t ssm = pass2_scatter_smem<K>(C1, F2);
+    FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_kernel<K>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ssm),
+          "smem attribute");
+    pass2_scatter_kernel<K><<<e->max_pieces, Pass2Shape<K>::kThreads, ssm, st>>>(
+        (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr, C1, F1,
+        F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, len, (int *)e->status.ptr);
+  }
+  FI_CK(cudaGetLastError(), "pass-2 scatter");
+  e->mark(4 + 4 * r, st);
+  e->launches += 4;
+  return FI_OK;
+}
 
+// Partitions relation r (0 = build, 1 = probe) into the layout the join
+// reads: one Contiguous pass into rel1[r]/off1[r], or two passes into
+// rel2[r]/off2[r].
+template <typename K>
+static int engine_partition(fi_radix_join_engine *e, int r, const K *key,
+                            const K *pay, uint64_t len, cudaStream_t st) {
+  const uint32_t C1 = e->C1, F1 = e->F1;
+  const uint32_t b1 = (uint32_t)e->bits1;
+  const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
+  if ((uint64_t)(len + C1 - 1) / C1 >= 0xffffffffull)
+    return set_error(FI_ERR_INTEGER_OVERFLOW, "relation too large");
+  if (e->bits2 < 0) {
+    const uint64_t padded = len + (uint64_t)F1 * pad;
+    FI_CK(launch_contiguous_prefix_sum<K>(
+              key, nullptr, len, C1, b1, 0, pad, nullptr, nullptr,
+              (uint64_t *)e->off1[r].ptr, (uint64_t *)e->loc1[r].ptr, 0,
+              e->hs(), e->sm_count, st),
+          "prefix sum");
+    e->mark(1 + 4 * r, st);
+    FI_CK(launch_partition<K>(key, pay, len, C1, b1, 0,
+                              (const uint64_t *)e->loc1[r].ptr, e->rel1[r].ptr,
+                              padded, e->scatter_variant(), (int *)e->status.ptr,
+                              st),
+          "partition");
+    e->mark(2 + 4 * r, st);
+    e->mark(3 + 4 * r, st);
+    e->mark(4 + 4 * r, st);
+    e->launches += 3;
+  } else {
+    const uint64_t padded1 = len + (uint64_t)C1 * F1 * pad;
+    FI_CK(launch_chunked_prefix_sum<K>(key, len, C1, b1, 0, pad,
+                                       (uint64_t *)e->off1[r].ptr, e->hs(),
+                                       e->sm_count, st),
+          "pass-1 prefix sum");
+    e->mark(1 + 4 * r, st);
+    FI_CK(launch_partition<K>(key, pay, len, C1, b1, 0,
+                              (const uint64_t *)e->off1[r].ptr, e->rel1[r].ptr,
+                              padded1, e->scatter_variant(), (int *)e->status.ptr,
+                              st),
+          "pass-1 partition");
+    e->mark(2 + 4 * r, st);
+    int rc = engine_pass2<K>(e, r, C1, padded1, len, st);
+    if (rc) return rc;
+    e->launches += (hist_splits(C1, e->sm_count) == 1 ? 1u : 2u) + 1;
+  }
+  e->part_len[r] = len;
+  return FI_OK;
+}
+
+// Joins the partitioned build and probe relations and writes {sum, count}
+// to the device `result`.
+template <typename K>
+static int engine_join(fi_radix_join_engine *e, fi_join_result *result,
+                       cudaStream_t st) {
   FI_CK(cudaMemsetAsync(e->join_sums.ptr, 0, e->join_sums.size, st), "memset");
   FI_CK(cudaMemsetAsync(e->join_count.ptr, 0, 8, st), "memset");
+  const int scheme = e->scheme == FI_HASHING_PERFECT ? 0 : 2;
   JoinScratch js{(uint32_t *)e->join_items.ptr, (uint32_t *)e->join_part.ptr,
                  (uint64_t *)e->join_tiles.ptr, (uint32_t *)e->join_counters.ptr,
                  (int *)e->status.ptr};
-  const uint32_t hist_launches = hist_splits(C1, e->sm_count) == 1 ? 1u : 2u;
-  e->launches = 0;
-  e->mark(0, st);
-
   if (e->bits2 < 0) {
-    // single pass: Contiguous layout (one chunk) for the join
-    uint64_t padded[2];
-    for (int r = 0; r < 2; ++r) {
-      padded[r] = lens[r] + (uint64_t)F1 * pad;
-      FI_CK(launch_contiguous_prefix_sum<K>(
-                keys[r], nullptr, lens[r], C1, b1, 0, pad, nullptr, nullptr,
-                (uint64_t *)e->off1[r].ptr, (uint64_t *)e->loc1[r].ptr, 0,
-                e->hs(), e->sm_count, st),
-            "prefix sum");
-      e->mark(1 + 4 * r, st);
-      FI_CK(launch_partition<K>(keys[r], pays[r], lens[r], C1, b1, 0,
-                                (const uint64_t *)e->loc1[r].ptr,
-                                e->rel1[r].ptr, padded[r], false,
-                                (int *)e->status.ptr, st),
-            "partition");
-      e->mark(2 + 4 * r, st);
-      e->mark(3 + 4 * r, st);
-      e->mark(4 + 4 * r, st);
-      e->launches += 3;
-    }
+    const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
+    const uint64_t padded[2] = {e->part_len[0] + (uint64_t)e->F1 * pad,
+                                e->part_len[1] + (uint64_t)e->F1 * pad};
     FI_CK(launch_radix_join<K>(e->rel1[0].ptr, (const uint64_t *)e->off1[0].ptr,
                                padded[0], pad, e->rel1[1].ptr,
                                (const uint64_t *)e->off1[1].ptr, padded[1], pad,
-                               F1, b1, scheme, e->join_grid(), kJoinBlock,
-                               (int64_t *)e->join_sums.ptr,
+                               e->F1, (uint32_t)e->bits1, scheme, e->join_grid(),
+                               e->join_block, (int64_t *)e->join_sums.ptr,
                                (uint64_t *)e->join_count.ptr, js, e->sm_count,
                                st),
           "join");
   } else {
-    const uint32_t b2 = (uint32_t)e->bits2;
-    const uint64_t mask2 = (uint64_t)(F2 - 1u) << b1;
-    for (int r = 0; r < 2; ++r) {
-      const uint64_t padded1 = lens[r] + (uint64_t)C1 * F1 * pad;
-      FI_CK(launch_chunked_prefix_sum<K>(keys[r], lens[r], C1, b1, 0, pad,
-                                         (uint64_t *)e->off1[r].ptr, e->hs(),
-                                         e->sm_count, st),
-            "pass-1 prefix sum");
-      e->mark(1 + 4 * r, st);
-      FI_CK(launch_partition<K>(keys[r], pays[r], lens[r], C1, b1, 0,
-                                (const uint64_t *)e->off1[r].ptr,
-                                e->rel1[r].ptr, padded1, false,
-                                (int *)e->status.ptr, st),
-            "pass-1 partition");
-      e->mark(2 + 4 * r, st);
-      Pass2Plan pl = e->plan(r);
-      pass2_plan_kernel<<<1, 1024, 0, st>>>((const uint64_t *)e->off1[r].ptr, C1,
-                                            F1, padded1, pad, pl,
-                                            (uint64_t *)e->piece_tmp[r].ptr);
-      FI_CK(cudaGetLastError(), "pass-2 plan");
-      piece_histogram_kernel<K><<<e->max_pieces, 512, F2 * 4, st>>>(
-          (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
-          C1, F1, F2, mask2, b1, pl);
-      FI_CK(cudaGetLastError(), "pass-2 histogram");
-      const size_t csm = (size_t)(F2 + 33) * 4;
-      pass2_cursor_kernel<<<F1, 1024, csm, st>>>(F1, F2, pl);
-      FI_CK(cudaGetLastError(), "pass-2 cursors");
-      e->mark(3 + 4 * r, st);
-      bool tma_done = false;
-      if constexpr (sizeof(Tuple<K>) == 16) {
-        // TMA-fed stages (the pass-1 relation is a 16-byte aligned
-        // allocation of 16-byte tuples, so every region segment qualifies)
-        const size_t tsm = pass2_tma_smem<K>(C1, F2);
-        if (tsm <= (size_t)device_max_smem_optin()) {
-          FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_tma_kernel<K>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tsm),
-                "smem attribute");
-          pass2_scatter_tma_kernel<K>
-              <<<e->max_pieces, TmaShape<K>::kThreads, tsm, st>>>(
-                  (const Tuple<K> *)e->rel1[r].ptr,
-                  (const uint64_t *)e->off1[r].ptr, C1, F1, F2, mask2, b1, pl,
-                  (Tuple<K> *)e->rel2[r].ptr, lens[r], (int *)e->status.ptr);
-          tma_done = true;
-        }
-      }
-      if (!tma_done) {
-        const size_t ssm = pass2_scatter_smem<K>(C1, F2);
-        FI_CK(cudaFuncSetAttribute((const void *)pass2_scatter_kernel<K>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)ssm),
-              "smem attribute");
-        pass2_scatter_kernel<K><<<e->max_pieces, Pass2Shape<K>::kThreads, ssm, st>>>(
-            (const Tuple<K> *)e->rel1[r].ptr, (const uint64_t *)e->off1[r].ptr,
-            C1, F1, F2, mask2, b1, pl, (Tuple<K> *)e->rel2[r].ptr, lens[r],
-            (int *)e->status.ptr);
-      }
-      FI_CK(cudaGetLastError(), "pass-2 scatter");
-      e->mark(4 + 4 * r, st);
-      e->launches += hist_launches + 1 + 4;
-    }
     FI_CK(launch_radix_join<K>(e->rel2[0].ptr, (const uint64_t *)e->off2[0].ptr,
-                               lens[0], 0, e->rel2[1].ptr,
-                               (const uint64_t *)e->off2[1].ptr, lens[1], 0,
-                               F1 * F2, b1 + b2, scheme, e->join_grid(),
-                               kJoinBlock, (int64_t *)e->join_sums.ptr,
+                               e->part_len[0], 0, e->rel2[1].ptr,
+                               (const uint64_t *)e->off2[1].ptr, e->part_len[1], 0,
+                               e->F1 * e->F2, (uint32_t)(e->bits1 + e->bits2),
+                               scheme, e->join_grid(), e->join_block,
+                               (int64_t *)e->join_sums.ptr,
                                (uint64_t *)e->join_count.ptr, js, e->sm_count,
                                st),
           "join");
   }
   e->mark(9, st);
   finish_result_kernel<<<1, 1024, 0, st>>>(
-      (const int64_t *)e->join_sums.ptr, (uint64_t)e->join_grid() * kJoinBlock,
+      (const int64_t *)e->join_sums.ptr, (uint64_t)e->join_grid() * e->join_block,
       (const uint64_t *)e->join_count.ptr, result);
-  e->launches += 3;  // join plan, join, result
   FI_CK(cudaGetLastError(), "result");
+  e->launches += 3;  // join plan, join, result
   e->mark(10, st);
   return FI_OK;
+}
+
+template <typename K>
+static int engine_check(fi_radix_join_engine *e, int r, const K *key,
+                        const K *pay, uint64_t len) {
+  if (!e) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  if (2 * sizeof(K) > e->tuple_bytes)
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "tuples larger than the engine was built for");
+  if (len > (r == 0 ? e->max_build : e->max_probe))
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "relation larger than the engine's workspace");
+  if (len > 0 && (!key || !pay))
+    return set_error(FI_ERR_INVALID_ARGUMENT, "null column");
+  return FI_OK;
+}
+
+template <typename K>
+static int engine_run(fi_radix_join_engine *e, const K *bk, const K *bp,
+                      uint64_t bn, const K *pk, const K *pp, uint64_t pn,
+                      fi_join_result *result, cudaStream_t st) {
+  int rc = engine_check<K>(e, 0, bk, bp, bn);
+  if (!rc) rc = engine_check<K>(e, 1, pk, pp, pn);
+  if (rc) return rc;
+  if (!result) return set_error(FI_ERR_INVALID_ARGUMENT, "null result");
+  e->launches = 0;
+  e->mark(0, st);
+  rc = engine_partition<K>(e, 0, bk, bp, bn, st);
+  if (!rc) rc = engine_partition<K>(e, 1, pk, pp, pn, st);
+  if (!rc) e->built = true;
+  if (!rc) rc = engine_join<K>(e, result, st);
+  return rc;
+}
+
+// Build once, probe many: the build relation stays partitioned in the
+// engine until the next build, and every probe joins a probe relation (or a
+// slice of one) against it.
+template <typename K>
+static int engine_build(fi_radix_join_engine *e, const K *key, const K *pay,
+                        uint64_t len, cudaStream_t st) {
+  int rc = engine_check<K>(e, 0, key, pay, len);
+  if (rc) return rc;
+  e->launches = 0;
+  e->mark(0, st);
+  rc = engine_partition<K>(e, 0, key, pay, len, st);
+  e->built = rc == FI_OK;
+  return rc;
+}
+
+template <typename K>
+static int engine_probe(fi_radix_join_engine *e, const K *key, const K *pay,
+                        uint64_t len, fi_join_result *result, cudaStream_t st) {
+  int rc = engine_check<K>(e, 1, key, pay, len);
+  if (rc) return rc;
+  if (!result) return set_error(FI_ERR_INVALID_ARGUMENT, "null result");
+  if (!e->built) return set_error(FI_ERR_INVALID_ARGUMENT, "probe before build");
+  e->launches = 0;
+  rc = engine_partition<K>(e, 1, key, pay, len, st);
+  if (!rc) rc = engine_join<K>(e, result, st);
+  return rc;
 }
 
 extern "C" int fi_radix_join_engine_set_events(fi_radix_join_engine *e,
@@ -656,4 +756,221 @@ extern "C" int fi_radix_join_engine_run_host_int64(
   }
   dres.release();
   return rc;
+}
+
+extern "C" int fi_radix_join_engine_build_int32(fi_radix_join_engine *e,
+                                                const int32_t *build_key,
+                                                const int32_t *build_pay,
+                                                uint64_t build_len,
+                                                fi_stream_t stream) {
+  return engine_build<int32_t>(e, build_key, build_pay, build_len,
+                               (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_build_int64(fi_radix_join_engine *e,
+                                                const int64_t *build_key,
+                                                const int64_t *build_pay,
+                                                uint64_t build_len,
+                                                fi_stream_t stream) {
+  return engine_build<int64_t>(e, build_key, build_pay, build_len,
+                               (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_probe_int32(
+    fi_radix_join_engine *e, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_probe<int32_t>(e, probe_key, probe_pay, probe_len, result,
+                               (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_probe_int64(
+    fi_radix_join_engine *e, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_probe<int64_t>(e, probe_key, probe_pay, probe_len, result,
+                               (cudaStream_t)stream);
+}
+
+// ---- per-run plan -------------------------------------------------------------
+extern "C" int fi_radix_join_engine_set_plan(fi_radix_join_engine *e,
+                                             const fi_join_plan *plan) {
+  if (!e || !plan) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  const int32_t b1 = plan->radix_bits.pass_bits[0];
+  const int32_t b2 = plan->radix_bits.pass_bits[1];
+  if (b1 < 0 || b1 > e->cap1 || plan->radix_bits.pass_bits[2] >= 0)
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "first-pass bits must lie in [0, %d], the engine's size",
+                     e->cap1);
+  if (b2 >= 0 && (e->cap2 < 0 || b2 > e->cap2))
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "second-pass bits exceed the engine's size");
+  if (plan->hashing_scheme != FI_HASHING_PERFECT &&
+      plan->hashing_scheme != FI_HASHING_BUCKET_CHAINING)
+    return set_error(FI_ERR_UNSUPPORTED,
+                     "the radix join supports Perfect and BucketChaining");
+  const uint32_t jb = plan->join_block ? plan->join_block : kJoinBlock;
+  if (jb != 256 && jb != 512 && jb != 1024)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "join_block must be 256, 512 or 1024");
+  if (plan->scatter > 1)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "unknown scatter variant");
+  e->bits1 = b1;
+  e->bits2 = b2;
+  e->F1 = 1u << b1;
+  e->F2 = b2 >= 0 ? (1u << b2) : 1u;
+  e->scheme = plan->hashing_scheme;
+  e->join_block = jb;
+  e->scatter = plan->scatter;
+  e->built = false;  // a resident build side used the old plan
+  return FI_OK;
+}
+
+// ---- out-of-core: first pass streamed from host memory ----------------------
+// The relations stay in host memory; pass 1 reads them over the host link
+// exactly once.  The input is cut into blocks of B tuples.  Block j is copied
+// into one of two device staging slots on a copy stream while the compute
+// stream partitions block j-1 out of the other slot, so the link and the
+// partitioning overlap.  Each block is partitioned on its own, with the
+// Contiguous layout over SM-count sub-chunks, into its own region of the
+// pass-1 relation: region base j*(B + F1*pad), i.e. the pass-1 relation is a
+// Chunked layout whose chunks are the blocks.  Pass 2 and the join then run
+// in HBM exactly as in the in-memory engine.  The nearest reference pieces
+// are the chunked multi-stream copy of numa-gpu/src/runtime/cuda.rs:891-985
+// and the cache-and-spill staging of gpu_triton_join.rs:391-470; the
+// reference has no streamed radix join.
+constexpr uint64_t kStreamBlockDefault = 1ull << 26;  // tuples per block
+constexpr uint64_t kStreamBlockAlign = 1ull << 16;
+
+template <typename K>
+static int engine_stream_pass1(fi_radix_join_engine *e, int r, const K *key,
+                               const K *pay, uint64_t len, uint64_t B,
+                               uint32_t nb, uint64_t *blk, cudaStream_t st) {
+  const uint32_t F1 = e->F1;
+  const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
+  const uint64_t padded1 = len + (uint64_t)nb * F1 * pad;
+  for (uint32_t j = 0; j < nb; ++j, ++*blk) {
+    const int slot = (int)(*blk & 1);
+    const uint64_t n = std::min<uint64_t>(B, len - (uint64_t)j * B);
+    K *sk = (K *)e->stage_key[slot].ptr, *sp = (K *)e->stage_pay[slot].ptr;
+    // the slot's previous block must be partitioned before the copy
+    // overwrites it
+    if (*blk >= 2)
+      FI_CK(cudaStreamWaitEvent(e->copy_stream, e->slot_free[slot], 0),
+            "stream wait");
+    FI_CK(cudaMemcpyAsync(sk, key + (uint64_t)j * B, n * sizeof(K),
+                          cudaMemcpyHostToDevice, e->copy_stream),
+          "host-to-device copy");
+    FI_CK(cudaMemcpyAsync(sp, pay + (uint64_t)j * B, n * sizeof(K),
+                          cudaMemcpyHostToDevice, e->copy_stream),
+          "host-to-device copy");
+    FI_CK(cudaEventRecord(e->slot_ready[slot], e->copy_stream), "event record");
+    FI_CK(cudaStreamWaitEvent(st, e->slot_ready[slot], 0), "stream wait");
+    FI_CK(launch_contiguous_prefix_sum<K>(
+              sk, nullptr, n, e->sm_count, (uint32_t)e->bits1, 0, pad, nullptr,
+              nullptr, (uint64_t *)e->off1[r].ptr + (uint64_t)j * F1,
+              (uint64_t *)e->stream_loc.ptr,
+              (uint64_t)j * (B + (uint64_t)F1 * pad), e->hs(), e->sm_count, st),
+          "pass-1 prefix sum");
+    FI_CK(launch_partition<K>(sk, sp, n, e->sm_count, (uint32_t)e->bits1, 0,
+                              (const uint64_t *)e->stream_loc.ptr,
+                              e->rel1[r].ptr, padded1, e->scatter_variant(),
+                              (int *)e->status.ptr, st),
+          "pass-1 partition");
+    FI_CK(cudaEventRecord(e->slot_free[slot], st), "event record");
+    e->launches += 3;
+  }
+  return FI_OK;
+}
+
+template <typename K>
+static int engine_run_streamed(fi_radix_join_engine *e, const K *bk,
+                               const K *bp, uint64_t bn, const K *pk,
+                               const K *pp, uint64_t pn, uint64_t block_tuples,
+                               fi_join_result *result, cudaStream_t st) {
+  int rc = engine_check<K>(e, 0, bk, bp, bn);
+  if (!rc) rc = engine_check<K>(e, 1, pk, pp, pn);
+  if (rc) return rc;
+  if (!result) return set_error(FI_ERR_INVALID_ARGUMENT, "null result");
+  if (e->bits2 < 0)
+    return set_error(FI_ERR_UNSUPPORTED,
+                     "the streamed join needs two radix passes (the first pass "
+                     "is partitioned block by block)");
+  uint64_t B = block_tuples ? block_tuples : kStreamBlockDefault;
+  B = (B + kStreamBlockAlign - 1) / kStreamBlockAlign * kStreamBlockAlign;
+  const uint64_t maxn = std::max(bn, pn);
+  if (maxn > 0 && B > maxn)
+    B = (maxn + kStreamBlockAlign - 1) / kStreamBlockAlign * kStreamBlockAlign;
+  const uint64_t lens[2] = {bn, pn};
+  uint32_t nb[2];
+  for (int r = 0; r < 2; ++r) {
+    const uint64_t blocks = (lens[r] + B - 1) / B;
+    if (blocks > e->C1)
+      return set_error(FI_ERR_INVALID_ARGUMENT,
+                       "block_tuples = %llu cuts a relation into %llu blocks; "
+                       "at most %u are supported, use larger blocks",
+                       (unsigned long long)B, (unsigned long long)blocks, e->C1);
+    nb[r] = (uint32_t)blocks;
+  }
+  if (bn == 0 || pn == 0) {
+    const fi_join_result zero{0, 0};
+    std::memcpy(result, &zero, sizeof zero);
+    return FI_OK;
+  }
+  // lazily set up the copy stream, events and staging slots
+  if (!e->copy_stream)
+    FI_CK(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking),
+          "stream create");
+  for (int i = 0; i < 2; ++i) {
+    if (!e->slot_ready[i])
+      FI_CK(cudaEventCreateWithFlags(&e->slot_ready[i], cudaEventDisableTiming),
+            "event create");
+    if (!e->slot_free[i])
+      FI_CK(cudaEventCreateWithFlags(&e->slot_free[i], cudaEventDisableTiming),
+            "event create");
+    rc = e->stage_key[i].reserve(B * sizeof(K), false);
+    if (!rc) rc = e->stage_pay[i].reserve(B * sizeof(K), false);
+    if (rc) return rc;
+  }
+  rc = e->stream_loc.reserve((size_t)e->sm_count * e->F1 * 8, false);
+  if (!rc) rc = e->result_dev.reserve(sizeof(fi_join_result), false);
+  if (rc) return rc;
+
+  e->launches = 0;
+  e->mark(0, st);
+  const K *keys[2] = {bk, pk}, *pays[2] = {bp, pp};
+  const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
+  uint64_t blk = 0;
+  for (int r = 0; r < 2; ++r) {
+    e->mark(1 + 4 * r, st);
+    rc = engine_stream_pass1<K>(e, r, keys[r], pays[r], lens[r], B, nb[r], &blk,
+                                st);
+    if (rc) return rc;
+    e->mark(2 + 4 * r, st);
+    const uint64_t padded1 = lens[r] + (uint64_t)nb[r] * e->F1 * pad;
+    rc = engine_pass2<K>(e, r, nb[r], padded1, lens[r], st);
+    if (rc) return rc;
+    e->part_len[r] = lens[r];
+  }
+  e->built = true;
+  rc = engine_join<K>(e, (fi_join_result *)e->result_dev.ptr, st);
+  if (rc) return rc;
+  FI_CK(cudaMemcpyAsync(result, e->result_dev.ptr, sizeof(fi_join_result),
+                        cudaMemcpyDeviceToHost, st),
+        "result copy");
+  FI_CK(cudaStreamSynchronize(st), "synchronize");
+  return FI_OK;
+}
+
+extern "C" int fi_radix_join_engine_run_streamed_int32(
+    fi_radix_join_engine *e, const int32_t *build_key, const int32_t *build_pay,
+    uint64_t build_len, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, uint64_t block_tuples, fi_join_result *result,
+    fi_stream_t stream) {
+  return engine_run_streamed<int32_t>(e, build_key, build_pay, build_len,
+                                      probe_key, probe_pay, probe_len,
+                                      block_tuples, result, (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_run_streamed_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, uint64_t block_tuples, fi_join_result *result,
+    fi_stream_t stream) {
+  return engine_run_streamed<int64_t>(e, build_key, build_pay, build_len,
+                                      probe_key, probe_pay, probe_len,
+                                      block_tuples, result, (cudaStream_t)stream);
 }

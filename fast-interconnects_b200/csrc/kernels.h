@@ -60,16 +60,22 @@ cudaError_t launch_prefix_sum_and_transform(
     uint64_t *offsets, uint64_t *local_offsets, HistScratch s,
     uint32_t sm_count, cudaStream_t stream);
 
+// Scatter variants: the shared-memory tile write-combining scatter, fed by
+// TMA bulk copies where the columns allow it (kScatterAuto) or by register
+// loads (kScatterRegisters), or the per-tuple atomic scatter (kScatterNC).
+constexpr int kScatterAuto = 0;
+constexpr int kScatterNC = 1;
+constexpr int kScatterRegisters = 2;
+
 // Scatter of columns into a partitioned relation.  cursors[c*F+p] is the
 // first slot of (chunk c, partition p); the input is split into `chunks`
-// canonical chunks.  nc selects the per-tuple atomic scatter instead of the
-// shared-memory tile write-combining scatter.
+// canonical chunks.
 template <typename K>
 cudaError_t launch_partition(const K *keys, const K *pays, uint64_t len,
                              uint32_t chunks, uint32_t radix_bits,
                              uint32_t ignore_bits, const uint64_t *cursors,
-                             void *out, uint64_t out_len, bool nc, int *status,
-                             cudaStream_t stream);
+                             void *out, uint64_t out_len, int variant,
+                             int *status, cudaStream_t stream);
 
 // Hierarchical (two-level) scatter for large fanouts: level 1 scatters by the
 // high half of the pass bits into `tmp` (same chunking), level 2 scatters

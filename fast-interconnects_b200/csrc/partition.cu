@@ -197,12 +197,12 @@ static cudaError_t launch_tile(const K *keys, const K *pays, uint64_t len,
                                uint32_t chunks, uint32_t radix_bits,
                                uint32_t ignore_bits, const uint64_t *cursors,
                                void *out, uint64_t out_len, int *status,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, bool allow_tma = true) {
   constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
   const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
   // TMA-fed stages when both columns are 16-byte aligned and the stages fit
   const size_t tma_sm = tma_scatter_smem<K>(1u << radix_bits);
-  if ((reinterpret_cast<uintptr_t>(keys) % 16) == 0 &&
+  if (allow_tma && (reinterpret_cast<uintptr_t>(keys) % 16) == 0 &&
       (reinterpret_cast<uintptr_t>(pays) % 16) == 0 &&
       tma_sm <= (size_t)device_max_smem_optin()) {
     cudaError_t e = cudaFuncSetAttribute(
@@ -223,10 +223,10 @@ template <typename K>
 cudaError_t launch_partition(const K *keys, const K *pays, uint64_t len,
                              uint32_t chunks, uint32_t radix_bits,
                              uint32_t ignore_bits, const uint64_t *cursors,
-                             void *out, uint64_t out_len, bool nc, int *status,
-                             cudaStream_t stream) {
+                             void *out, uint64_t out_len, int variant,
+                             int *status, cudaStream_t stream) {
   const uint32_t F = 1u << radix_bits;
-  if (nc) {
+  if (variant == kScatterNC) {
     constexpr uint64_t kAlignMask =
         ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
     const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
@@ -241,7 +241,8 @@ cudaError_t launch_partition(const K *keys, const K *pays, uint64_t len,
     return cudaGetLastError();
   }
   return launch_tile<K>(keys, pays, len, chunks, radix_bits, ignore_bits,
-                        cursors, out, out_len, status, stream);
+                        cursors, out, out_len, status, stream,
+                        variant != kScatterRegisters);
 }
 
 template <typename K>
@@ -276,7 +277,7 @@ cudaError_t launch_partition_hierarchical(
 #define FI_INSTANTIATE_PARTITION(K)                                            \
   template cudaError_t launch_partition<K>(                                    \
       const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t,            \
-      const uint64_t *, void *, uint64_t, bool, int *, cudaStream_t);          \
+      const uint64_t *, void *, uint64_t, int, int *, cudaStream_t);           \
   template cudaError_t launch_partition_hierarchical<K>(                       \
       const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t,            \
       const uint64_t *, void *, uint64_t, void *, uint64_t *, HistScratch,     \

@@ -152,6 +152,11 @@ class _JoinResultC(C.Structure):
     _fields_ = [("sum", C.c_int64), ("count", C.c_uint64)]
 
 
+class _JoinPlanC(C.Structure):
+    _fields_ = [("radix_bits", _RadixBitsC), ("hashing_scheme", C.c_int),
+                ("join_block", C.c_uint32), ("scatter", C.c_uint32)]
+
+
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
@@ -505,6 +510,46 @@ class RadixJoinEngine:
             self.h, _ptr(build_key), _ptr(build_pay),
             C.c_uint64(build_key.numel()), _ptr(probe_key), _ptr(probe_pay),
             C.c_uint64(probe_key.numel()), C.byref(res), _stream(stream)))
+        return res.sum, res.count
+
+    def set_plan(self, radix_bits, hashing_scheme=HashingScheme.BucketChaining,
+                 join_block=0, scatter=0):
+        """Plan of the following runs, within the engine's creation bits
+        (fi_radix_join_engine_set_plan)."""
+        plan = _JoinPlanC(radix_bits.c(), int(hashing_scheme), join_block, scatter)
+        _check(lib().fi_radix_join_engine_set_plan(self.h, C.byref(plan)))
+
+    def build(self, build_key, build_pay, stream=None):
+        """Partitions the build relation; it stays resident until the next
+        build or plan."""
+        f = getattr(lib(), "fi_radix_join_engine_build_" + _sfx(build_key.dtype))
+        _check(f(self.h, _ptr(build_key), _ptr(build_pay),
+                 C.c_uint64(build_key.numel()), _stream(stream)))
+
+    def probe_async(self, probe_key, probe_pay, result=None, stream=None):
+        """Joins a probe relation (or a slice) against the resident build
+        side; result (device int64[2]) = [sum, count] of this probe."""
+        result = self.result if result is None else result
+        f = getattr(lib(), "fi_radix_join_engine_probe_" + _sfx(probe_key.dtype))
+        _check(f(self.h, _ptr(probe_key), _ptr(probe_pay),
+                 C.c_uint64(probe_key.numel()), _ptr(result), _stream(stream)))
+        return result
+
+    def probe(self, probe_key, probe_pay, stream=None):
+        r = self.probe_async(probe_key, probe_pay, stream=stream).cpu()
+        return int(r[0]), int(r[1]) & ((1 << 64) - 1)
+
+    def run_streamed(self, build_key, build_pay, probe_key, probe_pay,
+                     block_tuples=0, stream=None):
+        """Out-of-core join: host (pinned) columns, the first pass streamed
+        over the host link in blocks of block_tuples (0 = library default);
+        (sum, count) out; synchronous."""
+        res = _JoinResultC()
+        f = getattr(lib(), "fi_radix_join_engine_run_streamed_" + _sfx(build_key.dtype))
+        _check(f(self.h, _ptr(build_key), _ptr(build_pay),
+                 C.c_uint64(build_key.numel()), _ptr(probe_key), _ptr(probe_pay),
+                 C.c_uint64(probe_key.numel()), C.c_uint64(block_tuples),
+                 C.byref(res), _stream(stream)))
         return res.sum, res.count
 
 

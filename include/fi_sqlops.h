@@ -363,6 +363,75 @@ void fi_radix_join_engine_free(fi_radix_join_engine *e);
 /* Device bytes the engine holds. */
 uint64_t fi_radix_join_engine_workspace_bytes(const fi_radix_join_engine *e);
 
+/* Execution plan of the following runs (no reference counterpart; the
+ * reference fixes bits, scheme and launch shape per call site).  The
+ * engine's buffers were sized for the radix bits given at creation; a plan
+ * may use fewer bits per pass, one pass instead of two, and tuples no
+ * larger than the creation's tuple_bytes.  join_block: threads per join CTA
+ * (256, 512 or 1024; 0 = 512).  scatter: 0 = tile scatter fed by TMA bulk
+ * copies where the columns allow it, 1 = fed by register loads.  Setting a
+ * plan drops a resident build side. */
+typedef struct {
+  fi_radix_bits radix_bits;
+  fi_hashing_scheme hashing_scheme;
+  uint32_t join_block;
+  uint32_t scatter;
+} fi_join_plan;
+int fi_radix_join_engine_set_plan(fi_radix_join_engine *e,
+                                  const fi_join_plan *plan);
+
+/* Build once, probe many (no reference counterpart; the reference
+ * re-partitions both relations on every gpu_radix_join call).  build
+ * partitions the build relation and keeps it resident in the engine until
+ * the next build or plan; every probe partitions a probe relation, or one
+ * slice of a larger one, and joins it against the resident build side,
+ * writing {sum, count} of that probe to the device `result`.  The sums and
+ * counts of the slices of one probe relation add up (wrapping) to the
+ * result of one run over the whole relation.  Device pointers; asynchronous
+ * on `stream`; build and probe must be ordered on the GPU by the caller. */
+int fi_radix_join_engine_build_int32(fi_radix_join_engine *e,
+                                     const int32_t *build_key,
+                                     const int32_t *build_pay,
+                                     uint64_t build_len, fi_stream_t stream);
+int fi_radix_join_engine_build_int64(fi_radix_join_engine *e,
+                                     const int64_t *build_key,
+                                     const int64_t *build_pay,
+                                     uint64_t build_len, fi_stream_t stream);
+int fi_radix_join_engine_probe_int32(fi_radix_join_engine *e,
+                                     const int32_t *probe_key,
+                                     const int32_t *probe_pay,
+                                     uint64_t probe_len,
+                                     fi_join_result *result,
+                                     fi_stream_t stream);
+int fi_radix_join_engine_probe_int64(fi_radix_join_engine *e,
+                                     const int64_t *probe_key,
+                                     const int64_t *probe_pay,
+                                     uint64_t probe_len,
+                                     fi_join_result *result,
+                                     fi_stream_t stream);
+
+/* Out-of-core join (no reference counterpart; the nearest reference pieces
+ * are the chunked multi-stream copy of numa-gpu/src/runtime/cuda.rs:891-985
+ * and the cache-and-spill staging of gpu_triton_join.rs:391-470).  The four
+ * columns stay in host memory (pinned for overlap).  The first radix pass
+ * streams them over the host link once, in blocks of `block_tuples` tuples
+ * (0 = 2^26; rounded up to a multiple of 2^16), with two device staging
+ * slots so that the copy of block j+1 overlaps the partitioning of block j.
+ * The partitioned relations, the second pass and the join stay in HBM.  A
+ * relation may span at most SM-count blocks.  The engine's plan must have
+ * two passes.  Same result as fi_radix_join_engine_run_*; `result` is host
+ * memory.  Synchronous. */
+int fi_radix_join_engine_run_streamed_int32(
+    fi_radix_join_engine *e, const int32_t *build_key, const int32_t *build_pay,
+    uint64_t build_len, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, uint64_t block_tuples, fi_join_result *result,
+    fi_stream_t stream);
+int fi_radix_join_engine_run_streamed_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, uint64_t block_tuples, fi_join_result *result,
+    fi_stream_t stream);
+
 /* gpu_radix_join over device-resident columns: prefix sum, partition (one
  * or two passes) and per-partition join, all enqueued on `stream`.
  * `result` is a device fi_join_result that receives the result (it is

@@ -271,3 +271,65 @@ def test_gpu_generator_matches_cpu(fi, oracle, ndt, tdt):
     fi.gen_zipf_foreign_keys(z, 100000, 1.5, 4, 9)
     zc = oracle.zipf_foreign_keys(n, 100000, 1.5, 4, 9, ndt)
     assert (to_host(z) == zc).mean() > 0.999
+
+
+@pytest.mark.parametrize("bits", [(7,), (6, 6)])
+@pytest.mark.parametrize("scheme", ["Perfect", "BucketChaining"])
+def test_engine_build_once_probe_slices(fi, oracle, bits, scheme):
+    """The build side stays partitioned across probes: the slices of S,
+    probed one by one, add up (wrapping) to the whole-S join."""
+    n_b, n_p = 1 << 20, 3 * (1 << 20) + 777
+    r_key = oracle.primary_keys(n_b, 61, np.int64)
+    s_key = oracle.uniform_foreign_keys(n_p, n_b, 62, np.int64)
+    s_pay = oracle.uniform_foreign_keys(n_p, 1 << 62, 63, np.int64)
+    e = fi.RadixJoinEngine(n_b, 1 << 20, torch.int64, fi.RadixBits(*bits),
+                           getattr(fi.HashingScheme, scheme))
+    dk, dp = to_dev(s_key), to_dev(s_pay)
+    e.build(to_dev(r_key), to_dev(r_key))
+    tot_s, tot_c = 0, 0
+    for lo in range(0, n_p, 1 << 20):
+        hi = min(n_p, lo + (1 << 20))
+        s, c = e.probe(dk[lo:hi], dp[lo:hi])
+        tot_s = (tot_s + s) & ((1 << 64) - 1)
+        tot_c += c
+    e.status()
+    exp_s, exp_c, _, _ = oracle.cpu_radix_join(
+        r_key, r_key.copy(), s_key, s_pay, bits[0],
+        bits[1] if len(bits) > 1 else 1, 8, use_reference=False)
+    assert tot_c == exp_c == n_p
+    assert tot_s == exp_s & ((1 << 64) - 1)
+
+
+def test_engine_plans_on_one_engine(fi, oracle):
+    """One engine sized for 10+10 bits runs every smaller plan (one or two
+    passes, both schemes, every join block and scatter variant, int32
+    tuples in an int64-sized engine) with the same result."""
+    n = 1 << 20
+    r_key = oracle.primary_keys(n, 71, np.int64)
+    s_key = oracle.uniform_foreign_keys(2 * n, n, 72, np.int64)
+    exp_s, exp_c, _, _ = oracle.cpu_radix_join(
+        r_key, r_key.copy(), s_key, s_key.copy(), 6, 6, 8, use_reference=False)
+    e = fi.RadixJoinEngine(n, 2 * n, torch.int64, fi.RadixBits(10, 10),
+                           fi.HashingScheme.BucketChaining)
+    rk, sk = to_dev(r_key), to_dev(s_key)
+    rk32, sk32 = rk.to(torch.int32), sk.to(torch.int32)
+    for bits in [(8,), (10,), (5, 4), (9, 9), (10, 10)]:
+        for scheme in ["Perfect", "BucketChaining"]:
+            for jb, sc in [(256, 0), (512, 1), (1024, 0)]:
+                e.set_plan(fi.RadixBits(*bits), getattr(fi.HashingScheme, scheme),
+                           join_block=jb, scatter=sc)
+                assert e.run(rk, rk, sk, sk) == (exp_s, exp_c)
+                s32, c32 = e.run(rk32, rk32, sk32, sk32)
+                assert (s32, c32) == (exp_s, exp_c)
+    with pytest.raises(fi.SqlOpsError) as ex:
+        e.set_plan(fi.RadixBits(11, 10))  # above the engine's first-pass size
+    assert ex.value.kind == "InvalidArgument"
+
+
+def test_engine_probe_before_build(fi):
+    e = fi.RadixJoinEngine(1024, 1024, torch.int64, fi.RadixBits(4),
+                           fi.HashingScheme.BucketChaining)
+    k = torch.arange(1024, dtype=torch.int64, device="cuda")
+    with pytest.raises(fi.SqlOpsError) as ex:
+        e.probe(k, k)
+    assert ex.value.kind == "InvalidArgument"
