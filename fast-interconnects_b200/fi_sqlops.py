@@ -553,6 +553,46 @@ class RadixJoinEngine:
         return res.sum, res.count
 
 
+class _BatchJobC(C.Structure):
+    _fields_ = [("build_key", C.c_void_p), ("build_pay", C.c_void_p),
+                ("probe_key", C.c_void_p), ("probe_pay", C.c_void_p),
+                ("build_len", C.c_uint64), ("probe_len", C.c_uint64),
+                ("radix_bits", C.c_int32)]
+
+
+class JoinBatch:
+    """Many small joins of one tuple type run at once (fi_join_batch_*)."""
+
+    def __init__(self, dtype, max_jobs=256, max_tuples=1 << 24):
+        self.dtype = dtype
+        self.h = C.c_void_p()
+        _check(lib().fi_join_batch_new(C.c_uint32(_tuple_bytes(dtype)),
+                                       C.c_uint32(max_jobs), C.c_uint64(max_tuples),
+                                       C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_join_batch_free(self.h)
+            self.h = None
+
+    def device_bytes(self):
+        lib().fi_join_batch_device_bytes.restype = C.c_uint64
+        return lib().fi_join_batch_device_bytes(self.h)
+
+    def run(self, jobs):
+        """jobs: list of (build_key, build_pay, probe_key, probe_pay[, bits])
+        device tensors; returns [(sum, count)] per job."""
+        arr = (_BatchJobC * max(len(jobs), 1))()
+        for i, j in enumerate(jobs):
+            bk, bp, pk, pp = j[:4]
+            bits = j[4] if len(j) > 4 else -1
+            arr[i] = _BatchJobC(_ptr(bk).value, _ptr(bp).value, _ptr(pk).value,
+                                _ptr(pp).value, bk.numel(), pk.numel(), bits)
+        res = (_JoinResultC * max(len(jobs), 1))()
+        _check(lib().fi_join_batch_run(self.h, arr, C.c_uint32(len(jobs)), res))
+        return [(res[i].sum, res[i].count) for i in range(len(jobs))]
+
+
 # ---------------------------------------------------------------------------
 # seeded generator
 # ---------------------------------------------------------------------------

@@ -465,6 +465,30 @@ int fi_radix_join_engine_run_host_int64(fi_radix_join_engine *e,
 /* Synchronises and reports (and clears) a device-side error of the engine. */
 int fi_radix_join_engine_status(fi_radix_join_engine *e);
 
+/* ---- batched small joins (no reference counterpart; the reference runs
+ *      one join per gpu_radix_join call) ---------------------------------- */
+
+/* A batch runs many small joins of one tuple type at once: one radix pass
+ * per job, all jobs' histograms, scans, scatters and per-partition joins as
+ * four kernels over the whole batch, replayed as one CUDA graph (the join
+ * kernel takes (job, partition) items from a device work queue).  A batch
+ * handle owns a partition arena of max_tuples tuples (build + probe of all
+ * jobs) and holds at most max_jobs (<= 1024) jobs. */
+typedef struct fi_join_batch fi_join_batch;
+typedef struct {
+  const void *build_key, *build_pay, *probe_key, *probe_pay; /* device */
+  uint64_t build_len, probe_len;
+  int32_t radix_bits; /* <= 12; -1 = chosen from build_len */
+} fi_batch_job;
+int fi_join_batch_new(uint32_t tuple_bytes, uint32_t max_jobs,
+                      uint64_t max_tuples, fi_join_batch **out);
+void fi_join_batch_free(fi_join_batch *b);
+uint64_t fi_join_batch_device_bytes(const fi_join_batch *b);
+/* Runs the jobs; results[i] (host) gets job i's {sum, count}.  Synchronous.
+ * Jobs beyond the batch's capacity fail with FI_ERR_CAPACITY. */
+int fi_join_batch_run(fi_join_batch *b, const fi_batch_job *jobs,
+                      uint32_t n_jobs, fi_join_result *results);
+
 /* Phase timing (no reference counterpart; the reference times its phases
  * with CUDA events in gpu_radix_join.rs:255-276,281-356,415-532).  When
  * `events` (cudaEvent_t[n_events], n_events >= FI_ENGINE_PHASE_EVENTS) is
