@@ -1,0 +1,615 @@
+// Join server: continuous batching of radix joins on one B200.
+//
+// No reference counterpart: the reference's execution method runs one join
+// per call with two reused StreamStates (gpu_radix_join.rs:51-68,321-396).
+// The server admits requests of uneven sizes as they arrive and keeps the
+// GPU busy with several of them at once:
+//
+//  * admission: a request is admitted when the device memory it needs (its
+//    relations, when the server holds them) fits the budget next to what is
+//    already reserved; the fixed part (engines, batch arenas) is reserved at
+//    start.  Requests are admitted in arrival order; one larger than the
+//    whole free budget fails with FI_ERR_CAPACITY.
+//  * loading: server-held relations (host or synthetic sources) come from
+//    the stream-ordered allocator and are copied or generated on a load
+//    stream; an event marks them ready.
+//  * small joins (|R| + |S| below small_tuples) queue for a batch runner of
+//    their key type.  A free runner takes the queue (up to its capacity)
+//    when the other runner of the type is idle, the queue holds a quarter
+//    of a batch, or its oldest job has waited batch_wait_us, and replays its
+//    captured graph.  Two runners per key type alternate, so a batch forms
+//    while the previous one runs.
+//  * large joins run on a worker: a resident engine on its own stream,
+//    planned by the autotuner, built once and probed in slices of
+//    probe_slice tuples.  Workers overlap with each other and with batches.
+//  * completion: the scheduler thread polls the done events, releases the
+//    reservation and the relations, and hands responses to waiters.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/fi_sqlops.h"
+#include "api_internal.h"
+#include "batch.h"
+#include "kernels.h"
+
+namespace fi {
+
+// The autotuner's model plan (autotune.cu).
+void autotune_model(uint64_t build_len, fi_tuned_plan *out);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double us_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::micro>(b - a).count();
+}
+
+struct Request {
+  fi_join_request req{};
+  fi_tuned_plan plan{};
+  uint64_t reserve = 0;        // bytes of the budget this request holds
+  void *owned[4] = {};         // server-held relation columns
+  const void *cols[4] = {};    // columns the join reads (device)
+  cudaEvent_t ready = nullptr; // relations loaded
+  bool small = false;
+  Clock::time_point t_submit, t_admit;
+  fi_join_response resp{};
+  bool done = false;
+};
+
+constexpr uint32_t kMaxSlices = 64;
+
+struct Worker {
+  fi_radix_join_engine *engine = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  fi_join_result *d_res = nullptr;  // [kMaxSlices]
+  fi_join_result *h_res = nullptr;  // pinned [kMaxSlices]
+  uint32_t slices = 0;
+  Request *req = nullptr;
+};
+
+struct Runner {
+  BatchRunner batch;
+  std::vector<Request *> jobs;
+};
+
+}  // namespace
+}  // namespace fi
+
+using namespace fi;
+
+struct fi_join_server {
+  fi_join_server_config cfg{};
+  int device = 0;
+  cudaStream_t load_stream = nullptr;
+  std::vector<Worker> workers;
+  std::vector<Runner> runners;  // [0,1]: int32 keys, [2,3]: int64 keys
+  uint64_t fixed = 0, reserved = 0, peak = 0;
+
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  std::thread sched;
+  uint64_t next_ticket = 1;
+  std::deque<Request *> pending;               // not yet admitted
+  std::deque<Request *> small_q[2];            // admitted small, per key type
+  std::deque<Request *> large_q;               // admitted large
+  std::unordered_map<uint64_t, Request *> all; // every uncollected request
+  fi_join_server_stats stats{};
+  int fatal = 0;                               // sticky CUDA error
+
+  void loop();
+  bool admit(Request *r);
+  void load(Request *r);
+  void release(Request *r);
+  bool dispatch_batches(Clock::time_point now);
+  bool dispatch_large();
+  bool complete();
+  void finish(Request *r, int status);
+  void teardown();
+};
+
+namespace {
+
+uint64_t key_bytes_of(const fi_join_request &q) { return q.tuple_bytes / 2; }
+
+int type_index(const fi_join_request &q) { return q.tuple_bytes == 16 ? 1 : 0; }
+
+// Device bytes of a request's relations when the server holds them.
+uint64_t relation_bytes(const fi_join_request &q) {
+  const uint64_t kb = key_bytes_of(q);
+  switch (q.source) {
+    case FI_SOURCE_HOST:
+      return 2 * kb * (q.build_len + q.probe_len);
+    case FI_SOURCE_SYNTHETIC:  // payload = key: one column per relation
+      return kb * (q.build_len + q.probe_len);
+    default:
+      return 0;
+  }
+}
+
+template <typename K>
+void generate(Request *r, cudaStream_t st) {
+  const fi_join_request &q = r->req;
+  launch_gen_primary_keys<K>((K *)r->owned[0], q.build_len, q.seed, (K)1, st);
+  if (q.zipf_s > 0)
+    launch_gen_zipf_fk<K>((K *)r->owned[1], q.probe_len, q.build_len, q.zipf_s,
+                          q.seed + 1, q.seed, (K)1, st);
+  else
+    launch_gen_uniform_fk<K>((K *)r->owned[1], q.probe_len, q.build_len,
+                             q.seed + 1, (K)1, st);
+}
+
+}  // namespace
+
+void fi_join_server::release(Request *r) {
+  for (void *&p : r->owned)
+    if (p) {
+      cudaFreeAsync(p, load_stream);
+      p = nullptr;
+    }
+  if (r->ready) {
+    cudaEventDestroy(r->ready);
+    r->ready = nullptr;
+  }
+  reserved -= r->reserve;
+  r->reserve = 0;
+}
+
+void fi_join_server::finish(Request *r, int status) {
+  release(r);
+  r->resp.status = status;
+  r->resp.latency_us = us_between(r->t_submit, Clock::now());
+  r->done = true;
+  ++stats.completed;
+  cv_done.notify_all();
+}
+
+void fi_join_server::load(Request *r) {
+  const fi_join_request &q = r->req;
+  const uint64_t kb = key_bytes_of(q);
+  if (q.source == FI_SOURCE_DEVICE) {
+    r->cols[0] = q.build_key; r->cols[1] = q.build_pay;
+    r->cols[2] = q.probe_key; r->cols[3] = q.probe_pay;
+    return;
+  }
+  const uint64_t lens[4] = {q.build_len, q.build_len, q.probe_len, q.probe_len};
+  const bool host = q.source == FI_SOURCE_HOST;
+  const int ncols = host ? 4 : 2;
+  for (int i = 0; i < ncols; ++i) {
+    const uint64_t n = host ? lens[i] : lens[2 * i];
+    if (cudaMallocAsync(&r->owned[i], std::max<uint64_t>(n, 1) * kb,
+                        load_stream) != cudaSuccess) {
+      cudaGetLastError();
+      fatal = set_error(FI_ERR_OUT_OF_MEMORY, "relation allocation failed");
+      return;
+    }
+  }
+  if (host) {
+    const void *src[4] = {q.build_key, q.build_pay, q.probe_key, q.probe_pay};
+    for (int i = 0; i < 4; ++i) {
+      if (lens[i])
+        cudaMemcpyAsync(r->owned[i], src[i], lens[i] * kb, cudaMemcpyHostToDevice,
+                        load_stream);
+      r->cols[i] = r->owned[i];
+    }
+  } else {
+    if (kb == 8)
+      generate<int64_t>(r, load_stream);
+    else
+      generate<int32_t>(r, load_stream);
+    r->cols[0] = r->cols[1] = r->owned[0];
+    r->cols[2] = r->cols[3] = r->owned[1];
+  }
+  cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
+  cudaEventRecord(r->ready, load_stream);
+}
+
+bool fi_join_server::admit(Request *r) {
+  const fi_join_request &q = r->req;
+  const uint64_t budget = cfg.hbm_budget_bytes;
+  const uint64_t need = relation_bytes(q);
+  if (fixed + need > budget) {
+    finish(r, set_error(FI_ERR_CAPACITY,
+                        "request needs %llu bytes, more than the free budget",
+                        (unsigned long long)need));
+    return true;
+  }
+  if (fixed + reserved + need > budget) return false;
+  reserved += need;
+  peak = std::max(peak, reserved);
+  r->reserve = need;
+  r->t_admit = Clock::now();
+  r->resp.queue_us = us_between(r->t_submit, r->t_admit);
+  fi_autotune_plan(q.tuple_bytes, q.build_len, q.probe_len, q.zipf_s > 0 ? 1 : 0,
+                   cfg.small_tuples, &r->plan);
+  r->small = r->plan.batched != 0 && q.build_len + q.probe_len <= cfg.batch_tuples;
+  if (!r->small) {
+    fi_tuned_plan &p = r->plan;
+    // within the workers' engines (12 + 10 bits); perfect hashing needs
+    // dense unique build keys, which only the synthetic source guarantees
+    if (p.batched || p.radix_bits.pass_bits[0] > 12 || p.radix_bits.pass_bits[1] > 10)
+      autotune_model(q.build_len, &p);
+    if (p.hashing_scheme == FI_HASHING_PERFECT && q.source != FI_SOURCE_SYNTHETIC)
+      p.hashing_scheme = FI_HASHING_BUCKET_CHAINING;
+  }
+  load(r);
+  if (r->small)
+    small_q[type_index(q)].push_back(r);
+  else
+    large_q.push_back(r);
+  return true;
+}
+
+bool fi_join_server::dispatch_batches(Clock::time_point now) {
+  bool progress = false;
+  for (int t = 0; t < 2; ++t) {
+    std::deque<Request *> &q = small_q[t];
+    for (int i = 0; i < 2 && !q.empty(); ++i) {
+      Runner &run = runners[2 * t + i];
+      if (run.batch.busy()) continue;
+      const bool other_busy = runners[2 * t + (1 - i)].batch.busy();
+      const bool full = q.size() >= std::max<uint32_t>(1, run.batch.max_jobs() / 4);
+      const bool old = us_between(q.front()->t_admit, now) >= cfg.batch_wait_us;
+      if (other_busy && !full && !old) continue;
+      std::vector<BatchJob> jobs;
+      run.jobs.clear();
+      uint64_t tuples = 0;
+      while (!q.empty() && jobs.size() < run.batch.max_jobs()) {
+        Request *r = q.front();
+        const uint64_t n = r->req.build_len + r->req.probe_len;
+        if (tuples + n > run.batch.max_tuples()) break;
+        tuples += n;
+        jobs.push_back(BatchJob{r->cols[0], r->cols[1], r->cols[2], r->cols[3],
+                                r->req.build_len, r->req.probe_len,
+                                (uint32_t)r->plan.radix_bits.pass_bits[0]});
+        run.jobs.push_back(r);
+        q.pop_front();
+        if (r->ready) cudaStreamWaitEvent(run.batch.stream(), r->ready, 0);
+      }
+      const int rc = run.batch.launch(jobs.data(), (uint32_t)jobs.size());
+      if (rc) {
+        for (Request *r : run.jobs) finish(r, rc);
+        run.jobs.clear();
+        continue;
+      }
+      run.batch.set_busy(true);
+      ++stats.batches;
+      stats.batched_jobs += jobs.size();
+      progress = true;
+    }
+  }
+  return progress;
+}
+
+static int run_large(Worker &w, Request *r, uint64_t slice) {
+  const fi_join_request &q = r->req;
+  const fi_tuned_plan &p = r->plan;
+  if (r->ready) {
+    cudaError_t ce = cudaStreamWaitEvent(w.stream, r->ready, 0);
+    if (ce != cudaSuccess) return cuda_error(ce, "stream wait");
+  }
+  fi_join_plan jp{p.radix_bits, p.hashing_scheme, p.join_block, p.scatter};
+  int rc = fi_radix_join_engine_set_plan(w.engine, &jp);
+  if (rc) return rc;
+  const uint64_t sn = q.probe_len;
+  if (sn > slice * kMaxSlices)
+    return set_error(FI_ERR_CAPACITY, "probe relation needs more than %u slices",
+                     kMaxSlices);
+  w.slices = sn ? (uint32_t)((sn + slice - 1) / slice) : 0;
+  fi_stream_t st = (fi_stream_t)w.stream;
+  if (q.tuple_bytes == 16) {
+    rc = fi_radix_join_engine_build_int64(w.engine, (const int64_t *)r->cols[0],
+                                          (const int64_t *)r->cols[1], q.build_len, st);
+    for (uint32_t s = 0; !rc && s < w.slices; ++s) {
+      const uint64_t o = (uint64_t)s * slice, n = std::min(slice, sn - o);
+      rc = fi_radix_join_engine_probe_int64(
+          w.engine, (const int64_t *)r->cols[2] + o, (const int64_t *)r->cols[3] + o,
+          n, w.d_res + s, st);
+    }
+  } else {
+    rc = fi_radix_join_engine_build_int32(w.engine, (const int32_t *)r->cols[0],
+                                          (const int32_t *)r->cols[1], q.build_len, st);
+    for (uint32_t s = 0; !rc && s < w.slices; ++s) {
+      const uint64_t o = (uint64_t)s * slice, n = std::min(slice, sn - o);
+      rc = fi_radix_join_engine_probe_int32(
+          w.engine, (const int32_t *)r->cols[2] + o, (const int32_t *)r->cols[3] + o,
+          n, w.d_res + s, st);
+    }
+  }
+  if (rc) return rc;
+  if (w.slices) {
+    cudaError_t ce = cudaMemcpyAsync(w.h_res, w.d_res, w.slices * sizeof(fi_join_result),
+                                     cudaMemcpyDeviceToHost, w.stream);
+    if (ce != cudaSuccess) return cuda_error(ce, "result copy");
+  }
+  cudaError_t ce = cudaEventRecord(w.done, w.stream);
+  if (ce != cudaSuccess) return cuda_error(ce, "event record");
+  return FI_OK;
+}
+
+bool fi_join_server::dispatch_large() {
+  bool progress = false;
+  for (Worker &w : workers) {
+    if (w.req || large_q.empty()) continue;
+    Request *r = large_q.front();
+    large_q.pop_front();
+    progress = true;
+    if (r->req.build_len > cfg.max_build) {
+      finish(r, set_error(FI_ERR_CAPACITY,
+                          "build relation above the server's max_build"));
+      continue;
+    }
+    const int rc = run_large(w, r, cfg.probe_slice);
+    if (rc) {
+      // the engine may hold work of this request: wait for it before the
+      // relations are released
+      cudaStreamSynchronize(w.stream);
+      finish(r, rc);
+    } else {
+      w.req = r;
+      ++stats.engine_runs;
+    }
+  }
+  return progress;
+}
+
+bool fi_join_server::complete() {
+  bool progress = false;
+  for (Worker &w : workers) {
+    if (!w.req) continue;
+    const cudaError_t ce = cudaEventQuery(w.done);
+    if (ce == cudaErrorNotReady) continue;
+    Request *r = w.req;
+    w.req = nullptr;
+    progress = true;
+    if (ce != cudaSuccess) {
+      fatal = cuda_error(ce, "large join");
+      finish(r, fatal);
+      continue;
+    }
+    uint64_t sum = 0, count = 0;
+    for (uint32_t s = 0; s < w.slices; ++s) {
+      sum += (uint64_t)w.h_res[s].sum;
+      count += w.h_res[s].count;
+    }
+    r->resp.result.sum = (int64_t)sum;
+    r->resp.result.count = count;
+    finish(r, fi_radix_join_engine_status(w.engine));
+  }
+  for (Runner &run : runners) {
+    if (!run.batch.busy()) continue;
+    const cudaError_t ce = cudaEventQuery(run.batch.done());
+    if (ce == cudaErrorNotReady) continue;
+    run.batch.set_busy(false);
+    progress = true;
+    const uint32_t n = (uint32_t)run.jobs.size();
+    const int st = ce == cudaSuccess ? FI_OK : (fatal = cuda_error(ce, "batch"));
+    for (uint32_t i = 0; i < n; ++i) {
+      Request *r = run.jobs[i];
+      r->resp.batched = 1;
+      r->resp.batch_jobs = n;
+      if (st == FI_OK) {
+        r->resp.result.sum = (int64_t)run.batch.results()[i].sum;
+        r->resp.result.count = run.batch.results()[i].count;
+      }
+      finish(r, st);
+    }
+    run.jobs.clear();
+  }
+  return progress;
+}
+
+void fi_join_server::loop() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lk(mu);
+  for (;;) {
+    bool progress = false;
+    while (!pending.empty() && !fatal) {
+      if (!admit(pending.front())) break;
+      pending.pop_front();
+      progress = true;
+    }
+    progress |= complete();
+    if (!fatal) {
+      progress |= dispatch_batches(Clock::now());
+      progress |= dispatch_large();
+    } else {
+      // a CUDA error is sticky: fail everything that has not started
+      for (std::deque<Request *> *q : {&pending, &small_q[0], &small_q[1], &large_q})
+        while (!q->empty()) {
+          finish(q->front(), fatal);
+          q->pop_front();
+        }
+    }
+    bool busy = false;
+    for (Worker &w : workers) busy |= w.req != nullptr;
+    for (Runner &r : runners) busy |= r.batch.busy();
+    const bool queued = !pending.empty() || !small_q[0].empty() ||
+                        !small_q[1].empty() || !large_q.empty();
+    if (stop && !busy && !queued) break;
+    if (!progress) {
+      // in-flight work is polled every 20 us; an idle server sleeps until a
+      // submit wakes it
+      if (busy || queued)
+        cv_work.wait_for(lk, std::chrono::microseconds(20));
+      else
+        cv_work.wait(lk);
+    }
+  }
+}
+
+void fi_join_server::teardown() {
+  for (Worker &w : workers) {
+    if (w.stream) cudaStreamSynchronize(w.stream);
+    if (w.engine) fi_radix_join_engine_free(w.engine);
+    if (w.d_res) cudaFree(w.d_res);
+    if (w.h_res) cudaFreeHost(w.h_res);
+    if (w.done) cudaEventDestroy(w.done);
+    if (w.stream) cudaStreamDestroy(w.stream);
+  }
+  workers.clear();
+  for (Runner &r : runners) r.batch.release();
+  runners.clear();
+  if (load_stream) {
+    cudaStreamSynchronize(load_stream);
+    cudaStreamDestroy(load_stream);
+  }
+  load_stream = nullptr;
+  for (auto &kv : all) delete kv.second;
+  all.clear();
+}
+
+// ---- C ABI ----------------------------------------------------------------------
+extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
+                                  fi_join_server **out) {
+  if (!out) return set_error(FI_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  auto *s = new fi_join_server();
+  if (cfg) s->cfg = *cfg;
+  fi_join_server_config &c = s->cfg;
+  if (!c.hbm_budget_bytes) c.hbm_budget_bytes = 150000000000ull;
+  if (!c.workers) c.workers = 2;
+  if (!c.small_tuples) c.small_tuples = 4ull << 20;
+  if (!c.max_batch_jobs) c.max_batch_jobs = 256;
+  if (!c.batch_tuples) c.batch_tuples = 1ull << 25;
+  if (!c.batch_wait_us) c.batch_wait_us = 200;
+  if (!c.max_build) c.max_build = 1ull << 28;
+  if (!c.probe_slice) c.probe_slice = 1ull << 28;
+  if (c.max_batch_jobs > kBatchMaxJobs || c.workers > 16) {
+    delete s;
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "at most %u jobs per batch and 16 workers", kBatchMaxJobs);
+  }
+  cudaGetDevice(&s->device);
+  int rc = FI_OK;
+  cudaError_t ce = cudaStreamCreateWithFlags(&s->load_stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
+  // keep freed relation memory in the stream-ordered pool for the next ones
+  cudaMemPool_t pool;
+  if (!rc && cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  s->workers.resize(rc ? 0 : c.workers);
+  for (Worker &w : s->workers) {
+    if (rc) break;
+    fi_radix_bits caps{{12, 10, -1}};
+    rc = fi_radix_join_engine_new(c.max_build, c.probe_slice, 16, caps,
+                                  FI_HASHING_BUCKET_CHAINING, &w.engine);
+    if (rc) break;
+    s->fixed += fi_radix_join_engine_workspace_bytes(w.engine);
+    if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) ||
+        (ce = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) ||
+        (ce = cudaMalloc((void **)&w.d_res, kMaxSlices * sizeof(fi_join_result))) ||
+        (ce = cudaHostAlloc((void **)&w.h_res, kMaxSlices * sizeof(fi_join_result),
+                            cudaHostAllocDefault)))
+      rc = cuda_error(ce, "worker set-up");
+  }
+  if (!rc) {
+    s->runners = std::vector<Runner>(4);
+    const uint32_t sm = (uint32_t)device_sm_count();
+    for (int i = 0; i < 4 && !rc; ++i) {
+      rc = s->runners[i].batch.init(i < 2 ? 4 : 8, c.max_batch_jobs, c.batch_tuples, sm);
+      s->fixed += s->runners[i].batch.device_bytes();
+    }
+  }
+  if (!rc && s->fixed > c.hbm_budget_bytes)
+    rc = set_error(FI_ERR_CAPACITY, "the engines and batch arenas (%llu bytes) "
+                   "exceed the budget", (unsigned long long)s->fixed);
+  if (rc) {
+    s->teardown();
+    delete s;
+    return rc;
+  }
+  s->stats.fixed_bytes = s->fixed;
+  s->sched = std::thread([s] { s->loop(); });
+  *out = s;
+  return FI_OK;
+}
+
+extern "C" void fi_join_server_free(fi_join_server *s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->sched.joinable()) s->sched.join();
+  s->teardown();
+  delete s;
+}
+
+extern "C" int fi_join_server_submit(fi_join_server *s, const fi_join_request *req,
+                                     uint64_t *ticket) {
+  if (!s || !req || !ticket) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  if (req->tuple_bytes != 8 && req->tuple_bytes != 16)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "tuple_bytes must be 8 or 16");
+  if (req->source > FI_SOURCE_SYNTHETIC)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "unknown source");
+  if (req->source != FI_SOURCE_SYNTHETIC &&
+      ((req->build_len && (!req->build_key || !req->build_pay)) ||
+       (req->probe_len && (!req->probe_key || !req->probe_pay))))
+    return set_error(FI_ERR_INVALID_ARGUMENT, "null column");
+  auto *r = new Request();
+  r->req = *req;
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->fatal) {
+      delete r;
+      return s->fatal;
+    }
+    *ticket = s->next_ticket++;
+    s->all[*ticket] = r;
+    s->pending.push_back(r);
+    ++s->stats.submitted;
+  }
+  s->cv_work.notify_one();
+  return FI_OK;
+}
+
+static int collect(fi_join_server *s, uint64_t ticket, fi_join_response *resp,
+                   bool block, int *done) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return set_error(FI_ERR_INVALID_ARGUMENT, "unknown ticket");
+  Request *r = it->second;
+  if (block) s->cv_done.wait(lk, [r] { return r->done; });
+  if (done) *done = r->done ? 1 : 0;
+  if (!r->done) return FI_OK;
+  *resp = r->resp;
+  s->all.erase(it);
+  delete r;
+  return FI_OK;
+}
+
+extern "C" int fi_join_server_wait(fi_join_server *s, uint64_t ticket,
+                                   fi_join_response *resp) {
+  if (!s || !resp) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  return collect(s, ticket, resp, true, nullptr);
+}
+
+extern "C" int fi_join_server_poll(fi_join_server *s, uint64_t ticket, int *done,
+                                   fi_join_response *resp) {
+  if (!s || !resp || !done) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  return collect(s, ticket, resp, false, done);
+}
+
+extern "C" int fi_join_server_stats_get(fi_join_server *s, fi_join_server_stats *out) {
+  if (!s || !out) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  out->reserved_bytes = s->reserved;
+  out->peak_reserved_bytes = s->peak;
+  return FI_OK;
+}

@@ -593,6 +593,128 @@ class JoinBatch:
         return [(res[i].sum, res[i].count) for i in range(len(jobs))]
 
 
+class _ServerConfigC(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("workers", C.c_uint32),
+                ("small_tuples", C.c_uint64), ("max_batch_jobs", C.c_uint32),
+                ("batch_tuples", C.c_uint64), ("batch_wait_us", C.c_uint32),
+                ("max_build", C.c_uint64), ("probe_slice", C.c_uint64)]
+
+
+class _RequestC(C.Structure):
+    _fields_ = [("tuple_bytes", C.c_uint32), ("source", C.c_uint32),
+                ("build_len", C.c_uint64), ("probe_len", C.c_uint64),
+                ("build_key", C.c_void_p), ("build_pay", C.c_void_p),
+                ("probe_key", C.c_void_p), ("probe_pay", C.c_void_p),
+                ("seed", C.c_uint64), ("zipf_s", C.c_double)]
+
+
+class _ResponseC(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batched", C.c_uint32),
+                ("result", _JoinResultC), ("batch_jobs", C.c_uint32),
+                ("reserved", C.c_uint32), ("queue_us", C.c_double),
+                ("latency_us", C.c_double)]
+
+
+class _ServerStatsC(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "submitted", "completed", "batches", "batched_jobs", "engine_runs",
+        "reserved_bytes", "peak_reserved_bytes", "fixed_bytes")]
+
+
+class JoinSource(enum.IntEnum):
+    Device = 0
+    Host = 1
+    Synthetic = 2
+
+
+class JoinServer:
+    """Continuous-batching join server (fi_join_server_*).  submit() returns
+    a ticket at once; wait()/poll() hand over a dict with status, sum,
+    count, batched, batch_jobs, queue_us and latency_us."""
+
+    def __init__(self, hbm_budget_bytes=0, workers=0, small_tuples=0,
+                 max_batch_jobs=0, batch_tuples=0, batch_wait_us=0, max_build=0,
+                 probe_slice=0):
+        cfg = _ServerConfigC(hbm_budget_bytes, workers, small_tuples, max_batch_jobs,
+                             batch_tuples, batch_wait_us, max_build, probe_slice)
+        self.h = C.c_void_p()
+        self._keep = {}
+        _check(lib().fi_join_server_new(C.byref(cfg), C.byref(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_join_server_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, tuple_bytes=16, source=JoinSource.Synthetic, build_len=0,
+               probe_len=0, columns=None, seed=0, zipf_s=0.0):
+        """columns: (build_key, build_pay, probe_key, probe_pay) tensors for
+        the device and host sources (kept alive until the response)."""
+        ptrs = [None] * 4
+        if columns is not None:
+            ptrs = [c.data_ptr() for c in columns]
+            build_len, probe_len = columns[0].numel(), columns[2].numel()
+        req = _RequestC(tuple_bytes, int(source), build_len, probe_len, *ptrs, seed,
+                        zipf_s)
+        t = C.c_uint64()
+        _check(lib().fi_join_server_submit(self.h, C.byref(req), C.byref(t)))
+        if columns is not None:
+            self._keep[t.value] = columns
+        return t.value
+
+    @staticmethod
+    def _resp(r):
+        return {"status": r.status, "sum": r.result.sum, "count": r.result.count,
+                "batched": bool(r.batched), "batch_jobs": r.batch_jobs,
+                "queue_us": r.queue_us, "latency_us": r.latency_us}
+
+    def wait(self, ticket):
+        r = _ResponseC()
+        _check(lib().fi_join_server_wait(self.h, C.c_uint64(ticket), C.byref(r)))
+        self._keep.pop(ticket, None)
+        return self._resp(r)
+
+    def poll(self, ticket):
+        r = _ResponseC()
+        done = C.c_int()
+        _check(lib().fi_join_server_poll(self.h, C.c_uint64(ticket), C.byref(done),
+                                         C.byref(r)))
+        if not done.value:
+            return None
+        self._keep.pop(ticket, None)
+        return self._resp(r)
+
+    def stats(self):
+        st = _ServerStatsC()
+        _check(lib().fi_join_server_stats_get(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in _ServerStatsC._fields_}
+
+
+class _TunedPlanC(C.Structure):
+    _fields_ = [("batched", C.c_uint32), ("radix_bits", _RadixBitsC),
+                ("hashing_scheme", C.c_int), ("join_block", C.c_uint32),
+                ("scatter", C.c_uint32)]
+
+
+def autotune_plan(tuple_bytes, build_len, probe_len, skew=0, small_tuples=0):
+    """The autotuner's plan as a dict (fi_autotune_plan)."""
+    p = _TunedPlanC()
+    _check(lib().fi_autotune_plan(C.c_uint32(tuple_bytes), C.c_uint64(build_len),
+                                  C.c_uint64(probe_len), C.c_uint32(skew),
+                                  C.c_uint64(small_tuples), C.byref(p)))
+    bits = [b for b in p.radix_bits.pass_bits if b >= 0]
+    return {"batched": bool(p.batched), "bits": tuple(bits),
+            "scheme": HashingScheme(p.hashing_scheme), "join_block": p.join_block,
+            "scatter": p.scatter}
+
+
+def autotune_load(path):
+    _check(lib().fi_autotune_load(None if path is None else path.encode()))
+
+
 # ---------------------------------------------------------------------------
 # seeded generator
 # ---------------------------------------------------------------------------

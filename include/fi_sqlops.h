@@ -532,6 +532,104 @@ int fi_datagen_zipf_foreign_keys_int64(int64_t *keys, uint64_t n,
 int fi_datagen_uniform_u64_keys(int64_t *keys, uint64_t n, uint64_t seed,
                                 fi_stream_t stream);
 
+/* ---- autotuner and join server (no reference counterpart; the nearest
+ *      reference pieces are the radix-bits heuristic of
+ *      scripts/benchmark_gpu_radix_join.py:92 and the two reused
+ *      StreamStates of gpu_radix_join.rs:51-68,321-396) ------------------ */
+
+/* What the autotuner chooses per (tuple type, |R|, |S|, skew). */
+typedef struct {
+  uint32_t batched;       /* 1: run in a batch of small joins */
+  fi_radix_bits radix_bits;
+  fi_hashing_scheme hashing_scheme;
+  uint32_t join_block;    /* threads per join CTA */
+  uint32_t scatter;       /* 0 TMA-fed tile scatter, 1 register-fed */
+} fi_tuned_plan;
+
+/* The plan for one join.  skew: 0 uniform probe keys, 1 skewed (Zipf).
+ * Joins below small_tuples (0 = 4M) tuples in total are batched.  Others
+ * use the nearest entry of the table loaded by fi_autotune_load (by tuple
+ * type, log2 |R|, log2 (|S|/|R|) and skew) or, without one, a model: about
+ * 4K build tuples per final partition, one pass up to 11 bits and two
+ * balanced passes above, bucket chaining, 512-thread join CTAs, TMA-fed
+ * scatters.  A table entry may name the perfect scheme, which is valid
+ * only for dense unique build keys. */
+int fi_autotune_plan(uint32_t tuple_bytes, uint64_t build_len,
+                     uint64_t probe_len, uint32_t skew, uint64_t small_tuples,
+                     fi_tuned_plan *out);
+/* Loads a measured table (text lines "tuple_bytes log2_build log2_ratio
+ * skew bits1 bits2 scheme join_block scatter", '#' comments), replacing
+ * the previous one; NULL clears it. */
+int fi_autotune_load(const char *path);
+
+typedef struct fi_join_server fi_join_server;
+
+typedef struct {
+  uint64_t hbm_budget_bytes; /* device memory the server may hold (0: 150e9) */
+  uint32_t workers;          /* concurrent large joins (0: 2) */
+  uint64_t small_tuples;     /* joins below this (|R|+|S|) are batched (0: 4M) */
+  uint32_t max_batch_jobs;   /* jobs per batch (0: 256) */
+  uint64_t batch_tuples;     /* partition arena of one batch (0: 2^25) */
+  uint32_t batch_wait_us;    /* longest wait for a fuller batch (0: 200) */
+  uint64_t max_build;        /* largest build relation (0: 2^28 tuples) */
+  uint64_t probe_slice;      /* probe tuples per engine probe (0: 2^28) */
+} fi_join_server_config;
+
+/* Where a request's relations come from. */
+typedef enum {
+  FI_SOURCE_DEVICE = 0,    /* device columns owned by the caller, ready when
+                              submitted and valid until the response */
+  FI_SOURCE_HOST = 1,      /* host columns: the server reserves device memory
+                              and copies them in */
+  FI_SOURCE_SYNTHETIC = 2  /* the server generates them: R keys a permutation
+                              of 1..|R| (seed), S keys foreign keys of R,
+                              uniform or Zipf(zipf_s) (seed + 1), payload =
+                              key */
+} fi_join_source;
+
+typedef struct {
+  uint32_t tuple_bytes; /* 8: (int32, int32); 16: (int64, int64) */
+  uint32_t source;      /* fi_join_source */
+  uint64_t build_len, probe_len;
+  const void *build_key, *build_pay, *probe_key, *probe_pay;
+  uint64_t seed;  /* FI_SOURCE_SYNTHETIC */
+  double zipf_s;  /* FI_SOURCE_SYNTHETIC; > 0 is also the autotuner's skew hint */
+} fi_join_request;
+
+typedef struct {
+  int32_t status;         /* FI_OK or the error of this request */
+  uint32_t batched;       /* 1: ran in a batch */
+  fi_join_result result;
+  uint32_t batch_jobs;    /* jobs in its batch */
+  uint32_t reserved;
+  double queue_us;        /* submit -> admitted (memory reserved) */
+  double latency_us;      /* submit -> result in host memory */
+} fi_join_response;
+
+typedef struct {
+  uint64_t submitted, completed, batches, batched_jobs, engine_runs;
+  uint64_t reserved_bytes, peak_reserved_bytes, fixed_bytes;
+} fi_join_server_stats;
+
+/* Starts a server on the current device: allocates the workers' engines and
+ * the batch runners (fixed_bytes of the budget) and a scheduler thread. */
+int fi_join_server_new(const fi_join_server_config *cfg, fi_join_server **out);
+/* Finishes the queued requests and releases everything. */
+void fi_join_server_free(fi_join_server *s);
+/* Queues one join and returns its ticket at once.  The scheduler admits it
+ * when its memory fits the budget, runs it (batched, or on a worker's
+ * engine, overlapping with other requests) and keeps the response until it
+ * is collected. */
+int fi_join_server_submit(fi_join_server *s, const fi_join_request *req,
+                          uint64_t *ticket);
+/* Blocks until the ticket's join is done; the response is handed over. */
+int fi_join_server_wait(fi_join_server *s, uint64_t ticket,
+                        fi_join_response *resp);
+/* Non-blocking: *done = 1 and the response handed over when finished. */
+int fi_join_server_poll(fi_join_server *s, uint64_t ticket, int *done,
+                        fi_join_response *resp);
+int fi_join_server_stats_get(fi_join_server *s, fi_join_server_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

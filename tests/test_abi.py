@@ -101,3 +101,28 @@ def test_errors_without_launch(fi):
                          4, 128)
     assert e.value.kind == "InvalidArgument"
     assert "pass is not specified" in str(e.value)
+
+
+def test_autotune_model_and_table(fi, tmp_path):
+    """The autotuner's model (no table) and a loaded table (no GPU needed)."""
+    fi.autotune_load(None)
+    p = fi.autotune_plan(16, 1 << 21, 1 << 22)
+    assert p["bits"] == (9,) and not p["batched"]          # 2^21 / 4096
+    p = fi.autotune_plan(16, 1 << 30, 1 << 30)
+    assert p["bits"] == (9, 9)                              # the 1024M join
+    p = fi.autotune_plan(8, 100_000, 400_000)
+    assert p["batched"] and p["bits"][0] <= 12              # below 4M tuples
+    assert not fi.autotune_plan(8, 100_000, 400_000, small_tuples=1000)["batched"]
+    table = tmp_path / "table.txt"
+    table.write_text("# tb log2r log2k skew b1 b2 scheme block scatter\n"
+                     "16 30 0 0 10 8 2 1024 1\n")
+    fi.autotune_load(str(table))
+    p = fi.autotune_plan(16, 1 << 30, 1 << 30)
+    assert p["bits"] == (10, 8) and p["join_block"] == 1024 and p["scatter"] == 1
+    assert fi.autotune_plan(16, 1 << 21, 1 << 22)["bits"] == (9,)  # too far
+    assert fi.autotune_plan(8, 1 << 30, 1 << 30)["bits"] == (9, 9)  # other type
+    table.write_text("16 30 0 0 10 8 2 333 1\n")
+    with pytest.raises(fi.SqlOpsError) as ex:
+        fi.autotune_load(str(table))
+    assert ex.value.kind == "InvalidArgument"
+    fi.autotune_load(None)
