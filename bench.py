@@ -55,8 +55,21 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
-                    choices=["join", "partition"],
-                    help="partition: the partition-only sweep")
+                    choices=["join", "partition", "ooc", "serve"],
+                    help="partition: the partition-only sweep; ooc: the "
+                         "out-of-core join from pinned host memory; serve: the "
+                         "join server against back-to-back plain calls")
+    ap.add_argument("--ooc-log2n", type=int, default=31,
+                    help="out-of-core join: |R| = |S| = 2^ooc_log2n int64 tuples")
+    ap.add_argument("--ooc-block", type=int, default=0,
+                    help="out-of-core join: tuples per streamed block (0 = default)")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-max-build", type=int, default=1 << 28,
+                    help="largest |R| of the served stream (log-uniform from 64K)")
+    ap.add_argument("--serve-load", type=float, default=1.0,
+                    help="arrival rate relative to the plain path's estimated "
+                         "capacity")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--sweep", default="6,8,10,12,14,16,18",
                     help="radix bits of the partition sweep")
     ap.add_argument("--part-log2n", type=int, default=29,
@@ -552,12 +565,294 @@ def run_partition_sweep(a):
         dist.destroy_process_group()
 
 
+def h2d_probe(torch, nbytes=1 << 30, reps=5):
+    """Pinned host-to-device copy bandwidth (GB/s): the host-link roofline."""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(reps):
+        d.copy_(h, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    gbs = nbytes * reps / (t0.elapsed_time(t1) / 1e3) / 1e9
+    del h, d
+    return gbs
+
+
+def run_ooc(a):
+    """Out-of-core join: R = S = 2^ooc_log2n (int64 key, int64 payload) in
+    pinned host memory (fewer if the host cannot hold them), R keys a
+    permutation of 1..N, S uniform foreign keys, payload = key in its own
+    column.  One step = one whole join with the first pass streamed over the
+    host link.  Reports tuples/s and host-link GB/s (16 B per tuple read
+    once over the link) against the measured pinned host-to-device copy."""
+    import psutil
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    log2n = a.ooc_log2n
+    avail = psutil.virtual_memory().available
+    while log2n > 20 and 4 * 8 * (1 << log2n) * 1.25 > avail:
+        log2n -= 1
+    n = 1 << log2n
+    seed = a.seed + 1000 * rank
+    host = []
+    for gen in ("pk", "fk"):
+        d = torch.empty(n, dtype=torch.int64, device="cuda")
+        if gen == "pk":
+            fi.gen_primary_keys(d, seed, base=1)
+        else:
+            fi.gen_uniform_foreign_keys(d, n, seed + 1, base=1)
+            expected_sum = int(d.sum().item())
+        for _ in range(2):  # key column, then payload = key
+            h = torch.empty(n, dtype=torch.int64, pin_memory=True)
+            h.copy_(d)
+            host.append(h)
+        del d
+    torch.cuda.empty_cache()
+    link = h2d_probe(torch)
+    engine = fi.RadixJoinEngine(n, n, torch.int64, fi.RadixBits(9, 9),
+                                fi.HashingScheme.BucketChaining)
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        s, c = engine.run_streamed(*host, block_tuples=a.ooc_block)
+        verified = verified and (c == n and s == expected_sum)
+    K = a.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(11)] for _ in range(K)]
+    wall = []
+    with ClockSampler(local) as clk:
+        for k in range(K):
+            engine.set_events(evs[k])
+            barrier(world)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s, c = engine.run_streamed(*host, block_tuples=a.ooc_block)
+            wall.append(time.perf_counter() - t0)
+            verified = verified and (c == n and s == expected_sum)
+    engine.set_events(None)
+    engine.status()
+    clocks = clk.summary()
+    dev_ms = max_over_ranks(statistics.mean(e[0].elapsed_time(e[10]) for e in evs),
+                            world)
+    stream_ms = statistics.mean(e[1].elapsed_time(e[2]) + e[5].elapsed_time(e[6])
+                                for e in evs)
+    link_bytes = 2 * n * 16
+    if rank == 0:
+        line = {"metric": "out-of-core radix join G tuples/s",
+                "value": world * 2 * n / (dev_ms / 1e3) / 1e9, "unit": "G tuples/s",
+                "n_gpus": world, "steps": K, "warmup": a.warmup,
+                "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded permutation PK 1..N, uniform FK, "
+                        "payload = key) in pinned host memory",
+                "config": {"workload": "ooc_radix_join_%dMx%dM_int64_9+9bits_uniform"
+                                       % (n >> 20, n >> 20),
+                           "tuples_per_relation": n, "requested_log2n": a.ooc_log2n,
+                           "block_tuples": a.ooc_block or (1 << 26),
+                           "host_bytes": 4 * 8 * n,
+                           "l2_flush": "none: inputs in host memory"},
+                "host_link": {"bytes_per_step": link_bytes,
+                              "achieved_gb_per_s": link_bytes / (dev_ms / 1e3) / 1e9,
+                              "peak_gb_per_s": link,
+                              "peak_source": "pinned cudaMemcpyAsync H2D, 1 GiB x 5",
+                              "frac": link_bytes / (dev_ms / 1e3) / 1e9 / link,
+                              "streamed_pass1_ms": stream_ms},
+                "wall_ms_per_step": 1e3 * statistics.mean(wall),
+                "gpu_launches": engine.last_launches() * K,
+                "clocks": clocks, "verified": bool(verified),
+                "workspace_gb": engine.workspace_bytes() / 1e9}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def serve_requests(a):
+    """The served-join stream: seeded Poisson arrivals; |R| log-uniform in
+    [64K, max], |S| = k |R| with k in {1,2,4,8,16}, int32 or int64 tuples,
+    S uniform or Zipf(1.0).  Arrival rate: a.serve_load times an estimate
+    of the plain path's capacity (40 G tuples/s plus 1 ms per call)."""
+    import numpy as np
+    rng = np.random.default_rng(a.seed)
+    reqs = []
+    lo, hi = np.log(64 << 10), np.log(a.serve_max_build)
+    for i in range(a.serve_requests):
+        rn = int(np.exp(rng.uniform(lo, hi)))
+        k = int(rng.choice([1, 2, 4, 8, 16]))
+        tb = int(rng.choice([8, 16]))
+        z = float(rng.choice([0.0, 1.0]))
+        reqs.append({"tb": tb, "rn": rn, "sn": k * rn, "seed": a.seed + 7 * i, "zipf": z})
+    est = sum((r["rn"] + r["sn"]) / 40e9 + 1e-3 for r in reqs)
+    rate = a.serve_load * len(reqs) / est
+    t = 0.0
+    for r in reqs:
+        t += rng.exponential(1.0 / rate)
+        r["arrival"] = t
+    return reqs, rate
+
+
+def pctl(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs), q))
+
+
+def run_plain_calls(fi, torch, reqs, max_build, slice_):
+    """Back-to-back plain calls: one request after the other on one reused
+    engine per tuple type (build once, probe slices), generating its
+    relations with the same kernels.  Returns per-request (result, service
+    seconds)."""
+    engines = {tb: fi.RadixJoinEngine(max_build, slice_,
+                                      torch.int64 if tb == 16 else torch.int32,
+                                      fi.RadixBits(12, 10),
+                                      fi.HashingScheme.BucketChaining)
+               for tb in (8, 16)}
+    out = []
+    for r in reqs:
+        dt = torch.int64 if r["tb"] == 16 else torch.int32
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rk = torch.empty(r["rn"], dtype=dt, device="cuda")
+        sk = torch.empty(r["sn"], dtype=dt, device="cuda")
+        fi.gen_primary_keys(rk, r["seed"])
+        if r["zipf"] > 0:
+            fi.gen_zipf_foreign_keys(sk, r["rn"], r["zipf"], r["seed"] + 1, r["seed"])
+        else:
+            fi.gen_uniform_foreign_keys(sk, r["rn"], r["seed"] + 1)
+        e = engines[r["tb"]]
+        p = fi.autotune_plan(r["tb"], r["rn"], r["sn"], 1 if r["zipf"] > 0 else 0,
+                             small_tuples=1)
+        e.set_plan(fi.RadixBits(*p["bits"]), p["scheme"], p["join_block"], p["scatter"])
+        e.build(rk, rk)
+        s_tot, c_tot = 0, 0
+        for o in range(0, r["sn"], slice_):
+            s, c = e.probe(sk[o:o + slice_], sk[o:o + slice_])
+            s_tot, c_tot = (s_tot + s) & ((1 << 64) - 1), c_tot + c
+        out.append(((s_tot, c_tot), time.perf_counter() - t0))
+        del rk, sk
+    e = None
+    engines.clear()
+    return out
+
+
+def run_serve(a):
+    """Served and batched joins against back-to-back plain calls on the same
+    request stream.  Plain: requests one after the other in arrival order
+    (start = max(arrival, previous finish)); served: a submitter thread
+    hands each request to the join server at its arrival time, the server
+    admits, batches and overlaps them.  Latency = completion - arrival;
+    throughput = all tuples / (last completion - first arrival)."""
+    import threading
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    reqs, rate = serve_requests(a)
+    slice_ = a.serve_max_build
+    tuples = sum(r["rn"] + r["sn"] for r in reqs)
+    # warm-up of both paths on a few requests (untimed)
+    warm = reqs[:max(a.warmup, 1)]
+    run_plain_calls(fi, torch, warm, a.serve_max_build, slice_)
+    torch.cuda.empty_cache()
+    # plain: measured service times on the arrival timeline
+    plain = run_plain_calls(fi, torch, reqs, a.serve_max_build, slice_)
+    torch.cuda.empty_cache()
+    finish, plain_lat = 0.0, []
+    for r, (_, svc) in zip(reqs, plain):
+        finish = max(r["arrival"], finish) + svc
+        plain_lat.append(finish - r["arrival"])
+    plain_span = finish - reqs[0]["arrival"]
+    # served
+    srv = fi.JoinServer(hbm_budget_bytes=int(a.serve_budget_gb * 1e9),
+                        max_build=a.serve_max_build, probe_slice=slice_)
+    for t in [srv.submit(tuple_bytes=r["tb"], build_len=r["rn"], probe_len=r["sn"],
+                         seed=r["seed"], zipf_s=r["zipf"]) for r in warm]:
+        srv.wait(t)
+    tickets = [None] * len(reqs)
+    lag = [0.0] * len(reqs)
+
+    def submitter(t_start):
+        for i, r in enumerate(reqs):
+            delay = t_start + r["arrival"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            lag[i] = time.perf_counter() - (t_start + r["arrival"])
+            tickets[i] = srv.submit(tuple_bytes=r["tb"], build_len=r["rn"],
+                                    probe_len=r["sn"], seed=r["seed"],
+                                    zipf_s=r["zipf"])
+
+    with ClockSampler(local) as clk:
+        t_start = time.perf_counter() + 0.05
+        th = threading.Thread(target=submitter, args=(t_start,))
+        th.start()
+        resp = []
+        for i in range(len(reqs)):
+            while tickets[i] is None:
+                time.sleep(50e-6)
+            resp.append(srv.wait(tickets[i]))
+        t_end = time.perf_counter()
+        th.join()
+    clocks = clk.summary()
+    stats = srv.stats()
+    srv.close()
+    served_lat = [g["latency_us"] / 1e6 + lag[i] for i, g in enumerate(resp)]
+    served_span = t_end - (t_start + reqs[0]["arrival"])
+    verified = all(g["status"] == 0 and (g["sum"] & ((1 << 64) - 1), g["count"]) ==
+                   p[0] and g["count"] == r["sn"]
+                   for g, p, r in zip(resp, plain, reqs))
+    small = [i for i, g in enumerate(resp) if g["batched"]]
+    if rank == 0:
+        line = {"metric": "served radix join G tuples/s",
+                "value": tuples / served_span / 1e9, "unit": "G tuples/s",
+                "n_gpus": world, "steps": len(reqs), "warmup": len(warm),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int32+int64",
+                "data": "synthetic (seeded Poisson stream; PK permutations, "
+                        "uniform/Zipf FK, payload = key)",
+                "config": {"workload": "served_joins_%d_requests" % len(reqs),
+                           "requests": len(reqs), "tuples": tuples,
+                           "max_build": a.serve_max_build,
+                           "arrival_rate_per_s": rate, "offered_load": a.serve_load,
+                           "hbm_budget_gb": a.serve_budget_gb,
+                           "l2_flush": "none: relations of most requests exceed L2"},
+                "served": {"g_tuples_per_s": tuples / served_span / 1e9,
+                           "makespan_s": served_span,
+                           "p50_ms": 1e3 * pctl(served_lat, 50),
+                           "p99_ms": 1e3 * pctl(served_lat, 99),
+                           "p999_ms": 1e3 * pctl(served_lat, 99.9),
+                           "small_p99_ms": 1e3 * pctl([served_lat[i] for i in small], 99)
+                           if small else None,
+                           "batched_requests": len(small), "batches": stats["batches"],
+                           "engine_runs": stats["engine_runs"],
+                           "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
+                           "fixed_gb": stats["fixed_bytes"] / 1e9},
+                "plain": {"g_tuples_per_s": tuples / plain_span / 1e9,
+                          "makespan_s": plain_span,
+                          "busy_g_tuples_per_s": tuples / sum(p[1] for p in plain) / 1e9,
+                          "p50_ms": 1e3 * pctl(plain_lat, 50),
+                          "p99_ms": 1e3 * pctl(plain_lat, 99),
+                          "p999_ms": 1e3 * pctl(plain_lat, 99.9),
+                          "small_p99_ms": 1e3 * pctl([plain_lat[i] for i in small], 99)
+                          if small else None},
+                "clocks": clocks, "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.workload == "partition":
         run_partition_sweep(a)
+    elif a.workload == "ooc":
+        run_ooc(a)
+    elif a.workload == "serve":
+        run_serve(a)
     else:
         run_ours(a)
 
