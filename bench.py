@@ -70,6 +70,8 @@ def parse():
                     help="arrival rate relative to the plain path's estimated "
                          "capacity")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-workers", type=int, default=1,
+                    help="engines of the server that run large joins at once")
     ap.add_argument("--sweep", default="6,8,10,12,14,16,18",
                     help="radix bits of the partition sweep")
     ap.add_argument("--part-log2n", type=int, default=29,
@@ -766,7 +768,8 @@ def run_serve(a):
     plain_span = finish - reqs[0]["arrival"]
     # served
     srv = fi.JoinServer(hbm_budget_bytes=int(a.serve_budget_gb * 1e9),
-                        max_build=a.serve_max_build, probe_slice=slice_)
+                        workers=a.serve_workers, max_build=a.serve_max_build,
+                        probe_slice=slice_)
     for t in [srv.submit(tuple_bytes=r["tb"], build_len=r["rn"], probe_len=r["sn"],
                          seed=r["seed"], zipf_s=r["zipf"]) for r in warm]:
         srv.wait(t)
@@ -816,6 +819,7 @@ def run_serve(a):
                            "max_build": a.serve_max_build,
                            "arrival_rate_per_s": rate, "offered_load": a.serve_load,
                            "hbm_budget_gb": a.serve_budget_gb,
+                           "server_workers": a.serve_workers,
                            "l2_flush": "none: relations of most requests exceed L2"},
                 "served": {"g_tuples_per_s": tuples / served_span / 1e9,
                            "makespan_s": served_span,

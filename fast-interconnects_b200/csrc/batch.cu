@@ -296,7 +296,7 @@ static size_t desc_bytes(uint32_t max_jobs) {
 }
 
 int BatchRunner::init(uint32_t key_bytes, uint32_t max_jobs,
-                      uint64_t max_tuples, uint32_t sm_count) {
+                      uint64_t max_tuples, uint32_t sm_count, int priority) {
   if (key_bytes != 4 && key_bytes != 8)
     return set_error(FI_ERR_INVALID_ARGUMENT, "key_bytes must be 4 or 8");
   if (max_jobs == 0 || max_jobs > kBatchMaxJobs)
@@ -311,7 +311,7 @@ int BatchRunner::init(uint32_t key_bytes, uint32_t max_jobs,
   sm_count_ = sm_count;
   max_counters_ = (uint64_t)max_jobs * 2u << kBatchMaxBits;
   const size_t db = desc_bytes(max_jobs);
-  FI_BCK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  FI_BCK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, priority));
   FI_BCK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
   void *p = nullptr;
   FI_BCK(cudaMalloc(&p, db));

@@ -56,9 +56,11 @@ uint32_t batch_bits(uint64_t build_len);
 
 class BatchRunner {
  public:
-  // key_bytes 4 or 8; allocates the arena and captures the graph.
+  // key_bytes 4 or 8; allocates the arena and captures the graph.  The
+  // runner's stream gets `priority` (cudaStreamCreateWithPriority; lower is
+  // more urgent, 0 the default).
   int init(uint32_t key_bytes, uint32_t max_jobs, uint64_t max_tuples,
-           uint32_t sm_count);
+           uint32_t sm_count, int priority = 0);
   void release();
   ~BatchRunner() { release(); }
 

@@ -473,6 +473,18 @@ extern "C" int fi_radix_join_engine_status(fi_radix_join_engine *e) {
   return read_and_clear_status(e->status);
 }
 
+extern "C" int fi_radix_join_engine_status_async(fi_radix_join_engine *e,
+                                                 int *host_status,
+                                                 fi_stream_t stream) {
+  if (!e || !host_status) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t ce = cudaMemcpyAsync(host_status, e->status.ptr, sizeof(int),
+                                   cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(e->status.ptr, 0, sizeof(int), st);
+  if (ce != cudaSuccess) return cuda_error(ce, "status copy");
+  return FI_OK;
+}
+
 #define FI_CK(expr, what)                                                      \
   do {                                                                         \
     cudaError_t e_ = (expr);                                                   \

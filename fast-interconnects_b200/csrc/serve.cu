@@ -59,6 +59,7 @@ struct Request {
   void *owned[4] = {};         // server-held relation columns
   const void *cols[4] = {};    // columns the join reads (device)
   cudaEvent_t ready = nullptr; // relations loaded
+  cudaStream_t load = nullptr; // stream that loaded (and frees) them
   bool small = false;
   Clock::time_point t_submit, t_admit;
   fi_join_response resp{};
@@ -72,7 +73,8 @@ struct Worker {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   fi_join_result *d_res = nullptr;  // [kMaxSlices]
-  fi_join_result *h_res = nullptr;  // pinned [kMaxSlices]
+  fi_join_result *h_res = nullptr;  // pinned [kMaxSlices + 1]; the engine's
+                                    // error word after the last slice
   uint32_t slices = 0;
   Request *req = nullptr;
 };
@@ -90,7 +92,9 @@ using namespace fi;
 struct fi_join_server {
   fi_join_server_config cfg{};
   int device = 0;
-  cudaStream_t load_stream = nullptr;
+  // relations of small joins load on a high-priority stream, so that they
+  // do not queue behind the generation or copy of a large one
+  cudaStream_t load_small = nullptr, load_large = nullptr;
   std::vector<Worker> workers;
   std::vector<Runner> runners;  // [0,1]: int32 keys, [2,3]: int64 keys
   uint64_t fixed = 0, reserved = 0, peak = 0;
@@ -154,7 +158,7 @@ void generate(Request *r, cudaStream_t st) {
 void fi_join_server::release(Request *r) {
   for (void *&p : r->owned)
     if (p) {
-      cudaFreeAsync(p, load_stream);
+      cudaFreeAsync(p, r->load);
       p = nullptr;
     }
   if (r->ready) {
@@ -184,6 +188,8 @@ void fi_join_server::load(Request *r) {
   }
   const uint64_t lens[4] = {q.build_len, q.build_len, q.probe_len, q.probe_len};
   const bool host = q.source == FI_SOURCE_HOST;
+  cudaStream_t load_stream = r->small ? load_small : load_large;
+  r->load = load_stream;
   const int ncols = host ? 4 : 2;
   for (int i = 0; i < ncols; ++i) {
     const uint64_t n = host ? lens[i] : lens[2 * i];
@@ -332,6 +338,9 @@ static int run_large(Worker &w, Request *r, uint64_t slice) {
                                      cudaMemcpyDeviceToHost, w.stream);
     if (ce != cudaSuccess) return cuda_error(ce, "result copy");
   }
+  // the engine's error word, without a device-wide synchronisation
+  rc = fi_radix_join_engine_status_async(w.engine, (int *)(w.h_res + kMaxSlices), st);
+  if (rc) return rc;
   cudaError_t ce = cudaEventRecord(w.done, w.stream);
   if (ce != cudaSuccess) return cuda_error(ce, "event record");
   return FI_OK;
@@ -384,7 +393,10 @@ bool fi_join_server::complete() {
     }
     r->resp.result.sum = (int64_t)sum;
     r->resp.result.count = count;
-    finish(r, fi_radix_join_engine_status(w.engine));
+    const int dev = *(const int *)(w.h_res + kMaxSlices);
+    finish(r, dev == 0 ? FI_OK
+                       : set_error(dev == FI_ERR_TIMEOUT ? FI_ERR_TIMEOUT : FI_ERR_RUNTIME,
+                                   "device-side error %d in a large join", dev));
   }
   for (Runner &run : runners) {
     if (!run.batch.busy()) continue;
@@ -460,11 +472,12 @@ void fi_join_server::teardown() {
   workers.clear();
   for (Runner &r : runners) r.batch.release();
   runners.clear();
-  if (load_stream) {
-    cudaStreamSynchronize(load_stream);
-    cudaStreamDestroy(load_stream);
-  }
-  load_stream = nullptr;
+  for (cudaStream_t *ls : {&load_small, &load_large})
+    if (*ls) {
+      cudaStreamSynchronize(*ls);
+      cudaStreamDestroy(*ls);
+      *ls = nullptr;
+    }
   for (auto &kv : all) delete kv.second;
   all.clear();
 }
@@ -492,7 +505,12 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   }
   cudaGetDevice(&s->device);
   int rc = FI_OK;
-  cudaError_t ce = cudaStreamCreateWithFlags(&s->load_stream, cudaStreamNonBlocking);
+  int prio_low = 0, prio_high = 0;  // numerically: least, greatest priority
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  cudaError_t ce = cudaStreamCreateWithPriority(&s->load_small,
+                                                cudaStreamNonBlocking, prio_high);
+  if (ce == cudaSuccess)
+    ce = cudaStreamCreateWithFlags(&s->load_large, cudaStreamNonBlocking);
   if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
   // keep freed relation memory in the stream-ordered pool for the next ones
   cudaMemPool_t pool;
@@ -511,7 +529,7 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
     if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) ||
         (ce = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) ||
         (ce = cudaMalloc((void **)&w.d_res, kMaxSlices * sizeof(fi_join_result))) ||
-        (ce = cudaHostAlloc((void **)&w.h_res, kMaxSlices * sizeof(fi_join_result),
+        (ce = cudaHostAlloc((void **)&w.h_res, (kMaxSlices + 1) * sizeof(fi_join_result),
                             cudaHostAllocDefault)))
       rc = cuda_error(ce, "worker set-up");
   }
@@ -519,7 +537,8 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
     s->runners = std::vector<Runner>(4);
     const uint32_t sm = (uint32_t)device_sm_count();
     for (int i = 0; i < 4 && !rc; ++i) {
-      rc = s->runners[i].batch.init(i < 2 ? 4 : 8, c.max_batch_jobs, c.batch_tuples, sm);
+      rc = s->runners[i].batch.init(i < 2 ? 4 : 8, c.max_batch_jobs, c.batch_tuples, sm,
+                                    prio_high);
       s->fixed += s->runners[i].batch.device_bytes();
     }
   }

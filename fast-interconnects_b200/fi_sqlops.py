@@ -25,6 +25,7 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfi_sqlops.so")
+TUNING_TABLE = os.path.join(HERE, "tuning_table.txt")
 
 PADDING_BYTES = 128
 ALIGN_BYTES = 128
@@ -66,6 +67,9 @@ def lib():
         _lib.fi_padding_len.restype = C.c_uint32
         _lib.fi_partitioned_relation_alloc_len.restype = C.c_uint64
         _lib.fi_radix_join_engine_workspace_bytes.restype = C.c_uint64
+        # the autotuner's measured table (autotune.py), when it exists
+        if os.path.exists(TUNING_TABLE):
+            _check(_lib.fi_autotune_load(TUNING_TABLE.encode()))
     return _lib
 
 

@@ -464,6 +464,12 @@ int fi_radix_join_engine_run_host_int64(fi_radix_join_engine *e,
 
 /* Synchronises and reports (and clears) a device-side error of the engine. */
 int fi_radix_join_engine_status(fi_radix_join_engine *e);
+/* The same without a device-wide synchronisation: enqueues on `stream` a
+ * copy of the engine's device error word (0 or an FI_ERR_* code) into the
+ * host int `host_status` (pinned, valid once the stream reaches it) and
+ * clears the word.  For callers that overlap engines with other work. */
+int fi_radix_join_engine_status_async(fi_radix_join_engine *e, int *host_status,
+                                      fi_stream_t stream);
 
 /* ---- batched small joins (no reference counterpart; the reference runs
  *      one join per gpu_radix_join call) ---------------------------------- */
