@@ -830,6 +830,9 @@ def run_serve(a):
                            if small else None,
                            "batched_requests": len(small), "batches": stats["batches"],
                            "engine_runs": stats["engine_runs"],
+                           "engine_busy_s": stats["engine_busy_us"] / 1e6,
+                           "batch_busy_s": stats["batch_busy_us"] / 1e6,
+                           "scheduler_enqueue_s": stats["enqueue_us"] / 1e6,
                            "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
                            "fixed_gb": stats["fixed_bytes"] / 1e9},
                 "plain": {"g_tuples_per_s": tuples / plain_span / 1e9,

@@ -712,6 +712,9 @@ extern "C" int fi_radix_join_engine_set_events(fi_radix_join_engine *e,
     return set_error(FI_ERR_INVALID_ARGUMENT, "need %d events",
                      FI_ENGINE_PHASE_EVENTS);
   for (int i = 0; i < FI_ENGINE_PHASE_EVENTS; ++i)
+    if (!events[i])
+      return set_error(FI_ERR_INVALID_ARGUMENT, "event %d is not a created event", i);
+  for (int i = 0; i < FI_ENGINE_PHASE_EVENTS; ++i)
     e->events[i] = (cudaEvent_t)events[i];
   e->record = true;
   return FI_OK;

@@ -11,9 +11,11 @@
 //    evict-first vector loads; counts go to a shared-memory histogram through
 //    plain shared atomics (the match.any aggregation of common.cuh measured
 //    slower on B200, even for Zipf-skewed keys).  Fanouts above 2^15 do not
-//    fit one CTA's shared memory: the bins are split into ranges of 2^15 and
-//    every (chunk, split) is read by one CTA per range, the CTAs adjacent in
-//    the grid so the repeated reads come from L2.  A chunk owned by a single
+//    fit one CTA's shared memory: a thread-block cluster of F/2^15 CTAs
+//    holds the histogram in distributed shared memory and every key is read
+//    once (histogram_cluster_kernel); where clusters cannot be scheduled the
+//    bins are split into ranges of 2^15 and every (chunk, split) is read by
+//    one CTA per range (histogram_kernel).  A chunk owned by a single
 //    CTA is scanned in place and its offsets written directly (one launch);
 //    otherwise the CTAs add their counts into a global per-chunk histogram
 //    and a second kernel scans it.
@@ -23,6 +25,8 @@
 //    (Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
 //    Look-back", 2016): tile ids are taken from an atomic counter so a tile
 //    only waits on tiles that are already running, and every wait is bounded.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -176,6 +180,54 @@ __global__ void __launch_bounds__(kHistThreads)
     for (uint32_t p = threadIdx.x; p < nbins; p += blockDim.x)
       if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
   }
+}
+
+// Histogram of fanouts above 2^15 with a thread-block cluster: the
+// cluster's R = F / 2^15 CTAs each hold 2^15 counters in shared memory, so
+// together they hold the whole histogram in distributed shared memory.
+// Every CTA reads its share of the (chunk, split) keys once and adds each
+// key to the counter of the CTA that owns its bin, through the cluster's
+// shared-memory window; then every CTA adds its own 2^15 counters to
+// g_hist.  Each key is read once from HBM (the bin-range kernel above reads
+// it R times).  Cluster barriers: after the counters are zeroed (before any
+// remote add) and after the adds (before the flush and before any CTA may
+// exit while its shared memory is still a target).
+constexpr uint32_t kClusterThreads = 1024;
+
+template <typename K>
+__global__ void __launch_bounds__(kClusterThreads)
+    histogram_cluster_kernel(const K *__restrict__ keys, uint64_t len,
+                             uint64_t clen, uint32_t chunks, uint32_t splits,
+                             uint32_t radix_bits, uint32_t ignore_bits,
+                             uint32_t *__restrict__ g_hist) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ uint32_t cnt[];  // [2^15]
+  constexpr uint32_t kBins = 1u << kHistSmemBinsLog2;
+  const uint32_t F = 1u << radix_bits;
+  const uint32_t R = cluster.num_blocks(), q = cluster.block_rank();
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  const uint32_t cid = blockIdx.x / R;  // (chunk, split) of this cluster
+  const uint32_t c = cid / splits, s = cid % splits;
+  uint64_t sb, se;
+  split_range<K>(len, clen, chunks, c, splits, s, sb, se);
+  // this CTA's share of the cluster's keys (16-byte aligned starts)
+  constexpr uint64_t kVec = 16 / sizeof(K);
+  const uint64_t per = ((se - sb + R - 1) / R + kVec - 1) / kVec * kVec;
+  const uint64_t qb = min(se, sb + per * q), qe = min(se, qb + per);
+  for (uint32_t i = threadIdx.x; i < kBins; i += blockDim.x) cnt[i] = 0;
+  cluster.sync();
+  for_each_key(keys, qb, qe, [&](K key, bool act) {
+    if (act) {
+      const uint32_t b = key_to_partition(key, mask, ignore_bits);
+      uint32_t *dst = cluster.map_shared_rank(cnt, b >> kHistSmemBinsLog2);
+      atomicAdd(dst + (b & (kBins - 1u)), 1u);
+    }
+  });
+  cluster.sync();
+  uint32_t *gh = g_hist + (uint64_t)c * F + (uint64_t)q * kBins;
+  for (uint32_t p = threadIdx.x; p < kBins; p += blockDim.x)
+    if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
 }
 
 // Per-chunk scan of g_hist into Chunked offsets (one CTA per chunk), in
@@ -409,6 +461,55 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
                               (int)bytes);
 }
 
+// Histogram of a fanout above 2^15 into g_hist (zeroed by the caller):
+// the cluster kernel when the GPU can schedule its clusters, else the
+// bin-range kernel.
+template <typename K>
+static cudaError_t launch_wide_histogram(const K *keys, const K *pays,
+                                         K *dst_key, K *dst_pay, uint64_t len,
+                                         uint64_t clen, uint32_t chunks,
+                                         uint32_t splits, uint32_t radix_bits,
+                                         uint32_t ignore_bits, uint32_t pad,
+                                         uint32_t *g_hist, cudaStream_t stream) {
+  const uint32_t ranges = hist_ranges(radix_bits);
+  if (dst_key == nullptr && ranges <= 8) {
+    const size_t csm = (size_t)sizeof(uint32_t) << kHistSmemBinsLog2;
+    cudaError_t e = cudaFuncSetAttribute(
+        (const void *)histogram_cluster_kernel<K>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+    if (e == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(chunks * splits * ranges);
+      cfg.blockDim = dim3(kClusterThreads);
+      cfg.dynamicSmemBytes = csm;
+      cfg.stream = stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = ranges;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      e = cudaOccupancyMaxActiveClusters(&clusters,
+                                         (const void *)histogram_cluster_kernel<K>,
+                                         &cfg);
+      if (e == cudaSuccess && clusters > 0)
+        return cudaLaunchKernelEx(&cfg, histogram_cluster_kernel<K>, keys, len,
+                                  clen, chunks, splits, radix_bits, ignore_bits,
+                                  g_hist);
+    }
+    cudaGetLastError();  // fall back to the bin ranges
+  }
+  const size_t sm = hist_smem(radix_bits);
+  cudaError_t e = set_smem<K>((const void *)histogram_kernel<K>, sm);
+  if (e != cudaSuccess) return e;
+  histogram_kernel<K><<<chunks * splits * ranges, kHistThreads, sm, stream>>>(
+      keys, pays, dst_key, dst_pay, len, clen, chunks, splits, ranges,
+      radix_bits, ignore_bits, pad, nullptr, g_hist);
+  return cudaGetLastError();
+}
+
 template <typename K>
 cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
                                       uint32_t chunks, uint32_t radix_bits,
@@ -431,10 +532,16 @@ cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
   }
   e = cudaMemsetAsync(s.hist, 0, (size_t)chunks * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  histogram_kernel<K><<<chunks * splits * ranges, kHistThreads, sm, stream>>>(
-      keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, ranges,
-      radix_bits, ignore_bits, pad, nullptr, s.hist);
-  e = cudaGetLastError();
+  if (ranges > 1) {
+    e = launch_wide_histogram<K>(keys, nullptr, nullptr, nullptr, len, clen,
+                                 chunks, splits, radix_bits, ignore_bits, pad,
+                                 s.hist, stream);
+  } else {
+    histogram_kernel<K><<<chunks * splits, kHistThreads, sm, stream>>>(
+        keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, 1,
+        radix_bits, ignore_bits, pad, nullptr, s.hist);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return e;
   const size_t ssm = scan_smem(F);
   e = set_smem<K>((const void *)chunked_scan_kernel, ssm);
@@ -482,9 +589,16 @@ cudaError_t launch_contiguous_prefix_sum(const K *keys, const K *pays,
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(s.hist, 0, (size_t)grid * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  histogram_kernel<K><<<grid * splits * ranges, kHistThreads, sm, stream>>>(
-      keys, pays, dst_key, dst_pay, len, clen, grid, splits, ranges,
-      radix_bits, ignore_bits, pad, nullptr, s.hist);
+  if (ranges > 1) {
+    e = launch_wide_histogram<K>(keys, pays, dst_key, dst_pay, len, clen, grid,
+                                 splits, radix_bits, ignore_bits, pad, s.hist,
+                                 stream);
+    if (e != cudaSuccess) return e;
+  } else {
+    histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
+        keys, pays, dst_key, dst_pay, len, clen, grid, splits, 1, radix_bits,
+        ignore_bits, pad, nullptr, s.hist);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_contiguous_scan(F, grid, pad, base, offsets, local_offsets, s,

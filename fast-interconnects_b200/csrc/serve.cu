@@ -5,14 +5,15 @@
 // The server admits requests of uneven sizes as they arrive and keeps the
 // GPU busy with several of them at once:
 //
-//  * admission: a request is admitted when the device memory it needs (its
-//    relations, when the server holds them) fits the budget next to what is
-//    already reserved; the fixed part (engines, batch arenas) is reserved at
-//    start.  Requests are admitted in arrival order; one larger than the
-//    whole free budget fails with FI_ERR_CAPACITY.
-//  * loading: server-held relations (host or synthetic sources) come from
-//    the stream-ordered allocator and are copied or generated on a load
-//    stream; an event marks them ready.
+//  * memory: the engines and batch arenas are allocated at start; the rest
+//    of the budget is one device slab for the relations the server holds,
+//    handed out by a host-side first-fit allocator, so admitting a request
+//    calls no CUDA allocator and frees nothing that the GPU still reads.
+//  * admission: a request is admitted when its relations (when the server
+//    holds them) get a block of the slab.  Requests are admitted in arrival
+//    order; one larger than the whole slab fails with FI_ERR_CAPACITY.
+//  * loading: server-held relations (host or synthetic sources) are copied
+//    or generated on a load stream; an event marks them ready.
 //  * small joins (|R| + |S| below small_tuples) queue for a batch runner of
 //    their key type.  A free runner takes the queue (up to its capacity)
 //    when the other runner of the type is idle, the queue holds a quarter
@@ -29,6 +30,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -56,7 +58,8 @@ struct Request {
   fi_join_request req{};
   fi_tuned_plan plan{};
   uint64_t reserve = 0;        // bytes of the budget this request holds
-  void *owned[4] = {};         // server-held relation columns
+  void *block = nullptr;       // its block of the relation arena
+  void *owned[4] = {};         // server-held relation columns (in block)
   const void *cols[4] = {};    // columns the join reads (device)
   cudaEvent_t ready = nullptr; // relations loaded
   cudaStream_t load = nullptr; // stream that loaded (and frees) them
@@ -71,7 +74,7 @@ constexpr uint32_t kMaxSlices = 64;
 struct Worker {
   fi_radix_join_engine *engine = nullptr;
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr, done = nullptr;  // timing events
   fi_join_result *d_res = nullptr;  // [kMaxSlices]
   fi_join_result *h_res = nullptr;  // pinned [kMaxSlices + 1]; the engine's
                                     // error word after the last slice
@@ -79,9 +82,56 @@ struct Worker {
   Request *req = nullptr;
 };
 
+// Host-side first-fit allocator over one device slab that holds the
+// relations of admitted requests: admission never calls the CUDA allocator,
+// and a block is only handed out again after the host has seen the work of
+// its previous owner complete.
+class Arena {
+ public:
+  static constexpr uint64_t kAlign = 256;
+  void init(void *base, uint64_t size) {
+    base_ = (unsigned char *)base;
+    free_.clear();
+    if (size) free_[0] = size;
+  }
+  void *alloc(uint64_t bytes) {
+    bytes = round(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const uint64_t off = it->first, left = it->second - bytes;
+      free_.erase(it);
+      if (left) free_[off + bytes] = left;
+      return base_ + off;
+    }
+    return nullptr;
+  }
+  void release(void *p, uint64_t bytes) {
+    uint64_t off = (uint64_t)((unsigned char *)p - base_), len = round(bytes);
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + len == next->first) {  // merge right
+      len += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {  // merge left
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += len;
+        return;
+      }
+    }
+    free_[off] = len;
+  }
+
+ private:
+  static uint64_t round(uint64_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
+  unsigned char *base_ = nullptr;
+  std::map<uint64_t, uint64_t> free_;  // offset -> length of free blocks
+};
+
 struct Runner {
   BatchRunner batch;
   std::vector<Request *> jobs;
+  cudaEvent_t start = nullptr, end = nullptr;  // timing events of a batch
 };
 
 }  // namespace
@@ -98,6 +148,9 @@ struct fi_join_server {
   std::vector<Worker> workers;
   std::vector<Runner> runners;  // [0,1]: int32 keys, [2,3]: int64 keys
   uint64_t fixed = 0, reserved = 0, peak = 0;
+  void *slab = nullptr;         // relation arena (budget - fixed, or less)
+  uint64_t slab_bytes = 0;
+  Arena arena;
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -156,11 +209,9 @@ void generate(Request *r, cudaStream_t st) {
 }  // namespace
 
 void fi_join_server::release(Request *r) {
-  for (void *&p : r->owned)
-    if (p) {
-      cudaFreeAsync(p, r->load);
-      p = nullptr;
-    }
+  if (r->block) arena.release(r->block, r->reserve);
+  r->block = nullptr;
+  for (void *&p : r->owned) p = nullptr;
   if (r->ready) {
     cudaEventDestroy(r->ready);
     r->ready = nullptr;
@@ -191,14 +242,11 @@ void fi_join_server::load(Request *r) {
   cudaStream_t load_stream = r->small ? load_small : load_large;
   r->load = load_stream;
   const int ncols = host ? 4 : 2;
+  unsigned char *at = (unsigned char *)r->block;
   for (int i = 0; i < ncols; ++i) {
     const uint64_t n = host ? lens[i] : lens[2 * i];
-    if (cudaMallocAsync(&r->owned[i], std::max<uint64_t>(n, 1) * kb,
-                        load_stream) != cudaSuccess) {
-      cudaGetLastError();
-      fatal = set_error(FI_ERR_OUT_OF_MEMORY, "relation allocation failed");
-      return;
-    }
+    r->owned[i] = at;
+    at += (n * kb + Arena::kAlign - 1) / Arena::kAlign * Arena::kAlign;
   }
   if (host) {
     const void *src[4] = {q.build_key, q.build_pay, q.probe_key, q.probe_pay};
@@ -222,15 +270,18 @@ void fi_join_server::load(Request *r) {
 
 bool fi_join_server::admit(Request *r) {
   const fi_join_request &q = r->req;
-  const uint64_t budget = cfg.hbm_budget_bytes;
-  const uint64_t need = relation_bytes(q);
-  if (fixed + need > budget) {
+  // columns rounded to the arena's alignment, at most four of them
+  const uint64_t need = relation_bytes(q) ? relation_bytes(q) + 4 * Arena::kAlign : 0;
+  if (need > slab_bytes) {
     finish(r, set_error(FI_ERR_CAPACITY,
                         "request needs %llu bytes, more than the free budget",
                         (unsigned long long)need));
     return true;
   }
-  if (fixed + reserved + need > budget) return false;
+  if (need) {
+    r->block = arena.alloc(need);
+    if (!r->block) return false;  // wait for memory to be released
+  }
   reserved += need;
   peak = std::max(peak, reserved);
   r->reserve = need;
@@ -282,7 +333,9 @@ bool fi_join_server::dispatch_batches(Clock::time_point now) {
         q.pop_front();
         if (r->ready) cudaStreamWaitEvent(run.batch.stream(), r->ready, 0);
       }
+      cudaEventRecord(run.start, run.batch.stream());
       const int rc = run.batch.launch(jobs.data(), (uint32_t)jobs.size());
+      cudaEventRecord(run.end, run.batch.stream());
       if (rc) {
         for (Request *r : run.jobs) finish(r, rc);
         run.jobs.clear();
@@ -304,6 +357,7 @@ static int run_large(Worker &w, Request *r, uint64_t slice) {
     cudaError_t ce = cudaStreamWaitEvent(w.stream, r->ready, 0);
     if (ce != cudaSuccess) return cuda_error(ce, "stream wait");
   }
+  cudaEventRecord(w.start, w.stream);
   fi_join_plan jp{p.radix_bits, p.hashing_scheme, p.join_block, p.scatter};
   int rc = fi_radix_join_engine_set_plan(w.engine, &jp);
   if (rc) return rc;
@@ -394,6 +448,9 @@ bool fi_join_server::complete() {
     r->resp.result.sum = (int64_t)sum;
     r->resp.result.count = count;
     const int dev = *(const int *)(w.h_res + kMaxSlices);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, w.start, w.done) == cudaSuccess)
+      stats.engine_busy_us += 1e3 * ms;
     finish(r, dev == 0 ? FI_OK
                        : set_error(dev == FI_ERR_TIMEOUT ? FI_ERR_TIMEOUT : FI_ERR_RUNTIME,
                                    "device-side error %d in a large join", dev));
@@ -404,6 +461,9 @@ bool fi_join_server::complete() {
     if (ce == cudaErrorNotReady) continue;
     run.batch.set_busy(false);
     progress = true;
+    float ms = 0.f;
+    if (ce == cudaSuccess && cudaEventElapsedTime(&ms, run.start, run.end) == cudaSuccess)
+      stats.batch_busy_us += 1e3 * ms;
     const uint32_t n = (uint32_t)run.jobs.size();
     const int st = ce == cudaSuccess ? FI_OK : (fatal = cuda_error(ce, "batch"));
     for (uint32_t i = 0; i < n; ++i) {
@@ -426,6 +486,7 @@ void fi_join_server::loop() {
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
     bool progress = false;
+    const Clock::time_point t0 = Clock::now();
     while (!pending.empty() && !fatal) {
       if (!admit(pending.front())) break;
       pending.pop_front();
@@ -435,7 +496,9 @@ void fi_join_server::loop() {
     if (!fatal) {
       progress |= dispatch_batches(Clock::now());
       progress |= dispatch_large();
-    } else {
+    }
+    if (progress) stats.enqueue_us += us_between(t0, Clock::now());
+    if (fatal) {
       // a CUDA error is sticky: fail everything that has not started
       for (std::deque<Request *> *q : {&pending, &small_q[0], &small_q[1], &large_q})
         while (!q->empty()) {
@@ -467,10 +530,15 @@ void fi_join_server::teardown() {
     if (w.d_res) cudaFree(w.d_res);
     if (w.h_res) cudaFreeHost(w.h_res);
     if (w.done) cudaEventDestroy(w.done);
+    if (w.start) cudaEventDestroy(w.start);
     if (w.stream) cudaStreamDestroy(w.stream);
   }
   workers.clear();
-  for (Runner &r : runners) r.batch.release();
+  for (Runner &r : runners) {
+    r.batch.release();
+    if (r.start) cudaEventDestroy(r.start);
+    if (r.end) cudaEventDestroy(r.end);
+  }
   runners.clear();
   for (cudaStream_t *ls : {&load_small, &load_large})
     if (*ls) {
@@ -480,6 +548,9 @@ void fi_join_server::teardown() {
     }
   for (auto &kv : all) delete kv.second;
   all.clear();
+  if (slab) cudaFree(slab);
+  slab = nullptr;
+  slab_bytes = 0;
 }
 
 // ---- C ABI ----------------------------------------------------------------------
@@ -512,12 +583,6 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   if (ce == cudaSuccess)
     ce = cudaStreamCreateWithFlags(&s->load_large, cudaStreamNonBlocking);
   if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
-  // keep freed relation memory in the stream-ordered pool for the next ones
-  cudaMemPool_t pool;
-  if (!rc && cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
   s->workers.resize(rc ? 0 : c.workers);
   for (Worker &w : s->workers) {
     if (rc) break;
@@ -527,7 +592,7 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
     if (rc) break;
     s->fixed += fi_radix_join_engine_workspace_bytes(w.engine);
     if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) ||
-        (ce = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) ||
+        (ce = cudaEventCreate(&w.done)) || (ce = cudaEventCreate(&w.start)) ||
         (ce = cudaMalloc((void **)&w.d_res, kMaxSlices * sizeof(fi_join_result))) ||
         (ce = cudaHostAlloc((void **)&w.h_res, (kMaxSlices + 1) * sizeof(fi_join_result),
                             cudaHostAllocDefault)))
@@ -539,18 +604,38 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
     for (int i = 0; i < 4 && !rc; ++i) {
       rc = s->runners[i].batch.init(i < 2 ? 4 : 8, c.max_batch_jobs, c.batch_tuples, sm,
                                     prio_high);
+      if (!rc && ((ce = cudaEventCreate(&s->runners[i].start)) ||
+                  (ce = cudaEventCreate(&s->runners[i].end))))
+        rc = cuda_error(ce, "event create");
       s->fixed += s->runners[i].batch.device_bytes();
     }
   }
   if (!rc && s->fixed > c.hbm_budget_bytes)
     rc = set_error(FI_ERR_CAPACITY, "the engines and batch arenas (%llu bytes) "
                    "exceed the budget", (unsigned long long)s->fixed);
+  if (!rc) {
+    // the relation arena: the rest of the budget, or what the device has
+    // free (less 1 GiB of headroom), whichever is smaller
+    size_t dev_free = 0, dev_total = 0;
+    cudaMemGetInfo(&dev_free, &dev_total);
+    uint64_t want = c.hbm_budget_bytes - s->fixed;
+    const uint64_t headroom = 1ull << 30;
+    if (dev_free > headroom && want > dev_free - headroom) want = dev_free - headroom;
+    want &= ~(Arena::kAlign - 1);
+    if (want && (ce = cudaMalloc(&s->slab, want)) != cudaSuccess)
+      rc = cuda_error(ce, "relation arena");
+    else {
+      s->slab_bytes = want;
+      s->arena.init(s->slab, want);
+    }
+  }
   if (rc) {
     s->teardown();
     delete s;
     return rc;
   }
   s->stats.fixed_bytes = s->fixed;
+  s->stats.arena_bytes = s->slab_bytes;
   s->sched = std::thread([s] { s->loop(); });
   *out = s;
   return FI_OK;

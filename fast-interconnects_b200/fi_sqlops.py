@@ -484,6 +484,9 @@ class RadixJoinEngine:
             _check(lib().fi_radix_join_engine_set_events(self.h, None, 0))
             self._events = None
             return
+        for e in events:  # torch creates an event's handle at its first record
+            if not e.cuda_event:
+                e.record()
         arr = (C.c_void_p * len(events))(*[e.cuda_event for e in events])
         self._events = (events, arr)
         _check(lib().fi_radix_join_engine_set_events(self.h, arr, len(events)))
@@ -622,7 +625,8 @@ class _ResponseC(C.Structure):
 class _ServerStatsC(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "submitted", "completed", "batches", "batched_jobs", "engine_runs",
-        "reserved_bytes", "peak_reserved_bytes", "fixed_bytes")]
+        "reserved_bytes", "peak_reserved_bytes", "fixed_bytes", "arena_bytes")] + [
+        (n, C.c_double) for n in ("engine_busy_us", "batch_busy_us", "enqueue_us")]
 
 
 class JoinSource(enum.IntEnum):

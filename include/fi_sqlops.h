@@ -571,7 +571,10 @@ int fi_autotune_load(const char *path);
 typedef struct fi_join_server fi_join_server;
 
 typedef struct {
-  uint64_t hbm_budget_bytes; /* device memory the server may hold (0: 150e9) */
+  uint64_t hbm_budget_bytes; /* device memory the server may hold (0: 150e9):
+                                the workers' engines, the batch arenas and a
+                                slab for the relations it holds (the rest,
+                                capped by the device's free memory) */
   uint32_t workers;          /* concurrent large joins (0: 2) */
   uint64_t small_tuples;     /* joins below this (|R|+|S|) are batched (0: 4M) */
   uint32_t max_batch_jobs;   /* jobs per batch (0: 256) */
@@ -615,6 +618,10 @@ typedef struct {
 typedef struct {
   uint64_t submitted, completed, batches, batched_jobs, engine_runs;
   uint64_t reserved_bytes, peak_reserved_bytes, fixed_bytes;
+  uint64_t arena_bytes;   /* device slab for the relations the server holds */
+  double engine_busy_us;  /* device time of the large joins (events) */
+  double batch_busy_us;   /* device time of the batches (events) */
+  double enqueue_us;      /* host time the scheduler spent issuing work */
 } fi_join_server_stats;
 
 /* Starts a server on the current device: allocates the workers' engines and
