@@ -11,11 +11,12 @@
 //    evict-first vector loads; counts go to a shared-memory histogram through
 //    plain shared atomics (the match.any aggregation of common.cuh measured
 //    slower on B200, even for Zipf-skewed keys).  Fanouts above 2^15 do not
-//    fit one CTA's shared memory: a thread-block cluster of F/2^15 CTAs
-//    holds the histogram in distributed shared memory and every key is read
-//    once (histogram_cluster_kernel); where clusters cannot be scheduled the
-//    bins are split into ranges of 2^15 and every (chunk, split) is read by
-//    one CTA per range (histogram_kernel).  A chunk owned by a single
+//    fit one CTA's shared memory: the bins are split into ranges of 2^15
+//    and every (chunk, split) is read by one CTA per range (histogram_kernel),
+//    the CTAs adjacent in the grid so the repeated reads mostly come from L2;
+//    at 2^18 bins a thread-block cluster of 8 CTAs holds the histogram in
+//    distributed shared memory and every key is read once
+//    (histogram_cluster_kernel).  A chunk owned by a single
 //    CTA is scanned in place and its offsets written directly (one launch);
 //    otherwise the CTAs add their counts into a global per-chunk histogram
 //    and a second kernel scans it.
@@ -472,7 +473,11 @@ static cudaError_t launch_wide_histogram(const K *keys, const K *pays,
                                          uint32_t ignore_bits, uint32_t pad,
                                          uint32_t *g_hist, cudaStream_t stream) {
   const uint32_t ranges = hist_ranges(radix_bits);
-  if (dst_key == nullptr && ranges <= 8) {
+  // measured on B200, 512M keys over 148 chunks: at 2^16 bins the two-range
+  // kernel takes 2.0 ms and the cluster 3.0 ms (its remote shared-memory
+  // atomics cost more than the second, mostly L2-served, key read); at 2^18
+  // bins eight reads per key make the ranges slower (7.8 ms vs 7.0 ms)
+  if (dst_key == nullptr && ranges == 8) {
     const size_t csm = (size_t)sizeof(uint32_t) << kHistSmemBinsLog2;
     cudaError_t e = cudaFuncSetAttribute(
         (const void *)histogram_cluster_kernel<K>,
