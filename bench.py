@@ -66,8 +66,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-max-build", type=int, default=1 << 28,
                     help="largest |R| of the served stream (log-uniform from 64K)")
-    ap.add_argument("--serve-load", type=float, default=1.0,
-                    help="arrival rate relative to the plain path's estimated "
+    ap.add_argument("--serve-load", type=float, default=0.8,
+                    help="arrival rate relative to the plain path's measured "
                          "capacity")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-workers", type=int, default=1,
@@ -674,10 +674,9 @@ def run_ooc(a):
 
 
 def serve_requests(a):
-    """The served-join stream: seeded Poisson arrivals; |R| log-uniform in
-    [64K, max], |S| = k |R| with k in {1,2,4,8,16}, int32 or int64 tuples,
-    S uniform or Zipf(1.0).  Arrival rate: a.serve_load times an estimate
-    of the plain path's capacity (40 G tuples/s plus 1 ms per call)."""
+    """The served-join stream: |R| log-uniform in [64K, max], |S| = k |R|
+    with k in {1,2,4,8,16}, int32 or int64 tuples, S uniform or Zipf(1.0),
+    all from a seed.  Arrivals are set by serve_arrivals."""
     import numpy as np
     rng = np.random.default_rng(a.seed)
     reqs = []
@@ -688,13 +687,20 @@ def serve_requests(a):
         tb = int(rng.choice([8, 16]))
         z = float(rng.choice([0.0, 1.0]))
         reqs.append({"tb": tb, "rn": rn, "sn": k * rn, "seed": a.seed + 7 * i, "zipf": z})
-    est = sum((r["rn"] + r["sn"]) / 40e9 + 1e-3 for r in reqs)
-    rate = a.serve_load * len(reqs) / est
+    return reqs
+
+
+def serve_arrivals(a, reqs, capacity_s):
+    """Seeded Poisson arrivals at a.serve_load times the plain path's
+    measured capacity (requests / sum of its service times)."""
+    import numpy as np
+    rng = np.random.default_rng(a.seed + 1)
+    rate = a.serve_load * len(reqs) / capacity_s
     t = 0.0
     for r in reqs:
         t += rng.exponential(1.0 / rate)
         r["arrival"] = t
-    return reqs, rate
+    return rate
 
 
 def pctl(xs, q):
@@ -751,16 +757,18 @@ def run_serve(a):
     import torch
     import fi_sqlops as fi
     world, rank, local = dist_setup(a.gpus)
-    reqs, rate = serve_requests(a)
+    reqs = serve_requests(a)
     slice_ = a.serve_max_build
     tuples = sum(r["rn"] + r["sn"] for r in reqs)
     # warm-up of both paths on a few requests (untimed)
     warm = reqs[:max(a.warmup, 1)]
     run_plain_calls(fi, torch, warm, a.serve_max_build, slice_)
     torch.cuda.empty_cache()
-    # plain: measured service times on the arrival timeline
+    # plain: measured service times, then the arrival timeline at a fraction
+    # of the plain path's capacity
     plain = run_plain_calls(fi, torch, reqs, a.serve_max_build, slice_)
     torch.cuda.empty_cache()
+    rate = serve_arrivals(a, reqs, sum(p[1] for p in plain))
     finish, plain_lat = 0.0, []
     for r, (_, svc) in zip(reqs, plain):
         finish = max(r["arrival"], finish) + svc

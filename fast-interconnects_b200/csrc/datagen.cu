@@ -73,10 +73,22 @@ __device__ __forceinline__ double dg_h_int_inv(double x, double s) {
   return exp(dg_helper1(t) * x);
 }
 
-__device__ uint64_t zipf_rank(uint64_t n, double s, uint64_t seed, uint64_t i) {
-  const double hx1 = dg_h_int(1.5, s) - 1.0;
-  const double hn = dg_h_int((double)n + 0.5, s);
-  const double sq = 2.0 - dg_h_int_inv(dg_h_int(2.5, s) - dg_h(2.0, s), s);
+// Constants of the rejection-inversion sampler for (n, s); computed once per
+// thread, outside the per-key loop.
+struct ZipfConst {
+  double hx1, hn, sq;
+};
+__device__ ZipfConst zipf_const(uint64_t n, double s) {
+  ZipfConst z;
+  z.hx1 = dg_h_int(1.5, s) - 1.0;
+  z.hn = dg_h_int((double)n + 0.5, s);
+  z.sq = 2.0 - dg_h_int_inv(dg_h_int(2.5, s) - dg_h(2.0, s), s);
+  return z;
+}
+
+__device__ uint64_t zipf_rank(uint64_t n, double s, const ZipfConst &z,
+                              uint64_t seed, uint64_t i) {
+  const double hx1 = z.hx1, hn = z.hn, sq = z.sq;
   for (uint64_t attempt = 0;; ++attempt) {
     uint64_t bits = dg_mix64(seed ^ dg_mix64(i * 64ull + attempt));
     double u01 = (double)(bits >> 11) * (1.0 / 9007199254740992.0);
@@ -109,9 +121,10 @@ __global__ void gen_uniform_fk_kernel(K *keys, uint64_t n, uint64_t pk_n,
 template <typename K>
 __global__ void gen_zipf_fk_kernel(K *keys, uint64_t n, uint64_t pk_n, double s,
                                    uint64_t seed, Perm p, K base) {
+  const ZipfConst z = zipf_const(pk_n, s);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
-    keys[i] = base + (K)perm_apply(p, zipf_rank(pk_n, s, seed, i) - 1);
+    keys[i] = base + (K)perm_apply(p, zipf_rank(pk_n, s, z, seed, i) - 1);
 }
 
 __global__ void gen_u64_kernel(int64_t *keys, uint64_t n, uint64_t seed) {
