@@ -13,7 +13,9 @@
 //    holds them) get a block of the slab.  Requests are admitted in arrival
 //    order; one larger than the whole slab fails with FI_ERR_CAPACITY.
 //  * loading: server-held relations (host or synthetic sources) are copied
-//    or generated on a load stream; an event marks them ready.
+//    or generated: those of small joins at admission on a high-priority load
+//    stream (an event marks them ready), those of large joins on their
+//    worker's stream just before the join.
 //  * small joins (|R| + |S| below small_tuples) queue for a batch runner of
 //    their key type.  A free runner takes the queue (up to its capacity)
 //    when the other runner of the type is idle, the queue holds a quarter
@@ -22,7 +24,10 @@
 //    while the previous one runs.
 //  * large joins run on a worker: a resident engine on its own stream,
 //    planned by the autotuner, built once and probed in slices of
-//    probe_slice tuples.  Workers overlap with each other and with batches.
+//    probe_slice tuples.  A free worker takes the shortest admitted large
+//    join.  Workers overlap with each other and with batches (one worker by
+//    default: two large joins at once each run at half speed, which only
+//    lengthens their latency).
 //  * completion: the scheduler thread polls the done events, releases the
 //    reservation and the relations, and hands responses to waiters.
 #include <algorithm>
@@ -144,7 +149,7 @@ struct fi_join_server {
   int device = 0;
   // relations of small joins load on a high-priority stream, so that they
   // do not queue behind the generation or copy of a large one
-  cudaStream_t load_small = nullptr, load_large = nullptr;
+  cudaStream_t load_small = nullptr;
   std::vector<Worker> workers;
   std::vector<Runner> runners;  // [0,1]: int32 keys, [2,3]: int64 keys
   uint64_t fixed = 0, reserved = 0, peak = 0;
@@ -166,7 +171,7 @@ struct fi_join_server {
 
   void loop();
   bool admit(Request *r);
-  void load(Request *r);
+  void load(Request *r, cudaStream_t stream);
   void release(Request *r);
   bool dispatch_batches(Clock::time_point now);
   bool dispatch_large();
@@ -229,7 +234,7 @@ void fi_join_server::finish(Request *r, int status) {
   cv_done.notify_all();
 }
 
-void fi_join_server::load(Request *r) {
+void fi_join_server::load(Request *r, cudaStream_t stream) {
   const fi_join_request &q = r->req;
   const uint64_t kb = key_bytes_of(q);
   if (q.source == FI_SOURCE_DEVICE) {
@@ -239,7 +244,7 @@ void fi_join_server::load(Request *r) {
   }
   const uint64_t lens[4] = {q.build_len, q.build_len, q.probe_len, q.probe_len};
   const bool host = q.source == FI_SOURCE_HOST;
-  cudaStream_t load_stream = r->small ? load_small : load_large;
+  cudaStream_t load_stream = stream;
   r->load = load_stream;
   const int ncols = host ? 4 : 2;
   unsigned char *at = (unsigned char *)r->block;
@@ -299,11 +304,14 @@ bool fi_join_server::admit(Request *r) {
     if (p.hashing_scheme == FI_HASHING_PERFECT && q.source != FI_SOURCE_SYNTHETIC)
       p.hashing_scheme = FI_HASHING_BUCKET_CHAINING;
   }
-  load(r);
-  if (r->small)
+  // small joins load now, on the high-priority stream, to be ready for the
+  // next batch; large ones load on their worker's stream when they run
+  if (r->small) {
+    load(r, load_small);
     small_q[type_index(q)].push_back(r);
-  else
+  } else {
     large_q.push_back(r);
+  }
   return true;
 }
 
@@ -404,15 +412,24 @@ bool fi_join_server::dispatch_large() {
   bool progress = false;
   for (Worker &w : workers) {
     if (w.req || large_q.empty()) continue;
-    Request *r = large_q.front();
-    large_q.pop_front();
+    // shortest job first among the admitted large joins: a long join no
+    // longer holds up the many shorter ones behind it (arrivals below
+    // capacity bound the wait of the longest)
+    auto pick = large_q.begin();
+    for (auto it = large_q.begin(); it != large_q.end(); ++it)
+      if ((*it)->req.build_len + (*it)->req.probe_len <
+          (*pick)->req.build_len + (*pick)->req.probe_len)
+        pick = it;
+    Request *r = *pick;
+    large_q.erase(pick);
     progress = true;
     if (r->req.build_len > cfg.max_build) {
       finish(r, set_error(FI_ERR_CAPACITY,
                           "build relation above the server's max_build"));
       continue;
     }
-    const int rc = run_large(w, r, cfg.probe_slice);
+    load(r, w.stream);
+    const int rc = fatal ? fatal : run_large(w, r, cfg.probe_slice);
     if (rc) {
       // the engine may hold work of this request: wait for it before the
       // relations are released
@@ -540,12 +557,11 @@ void fi_join_server::teardown() {
     if (r.end) cudaEventDestroy(r.end);
   }
   runners.clear();
-  for (cudaStream_t *ls : {&load_small, &load_large})
-    if (*ls) {
-      cudaStreamSynchronize(*ls);
-      cudaStreamDestroy(*ls);
-      *ls = nullptr;
-    }
+  if (load_small) {
+    cudaStreamSynchronize(load_small);
+    cudaStreamDestroy(load_small);
+    load_small = nullptr;
+  }
   for (auto &kv : all) delete kv.second;
   all.clear();
   if (slab) cudaFree(slab);
@@ -562,7 +578,7 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   if (cfg) s->cfg = *cfg;
   fi_join_server_config &c = s->cfg;
   if (!c.hbm_budget_bytes) c.hbm_budget_bytes = 150000000000ull;
-  if (!c.workers) c.workers = 2;
+  if (!c.workers) c.workers = 1;
   if (!c.small_tuples) c.small_tuples = 4ull << 20;
   if (!c.max_batch_jobs) c.max_batch_jobs = 256;
   if (!c.batch_tuples) c.batch_tuples = 1ull << 25;
@@ -580,8 +596,6 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   cudaError_t ce = cudaStreamCreateWithPriority(&s->load_small,
                                                 cudaStreamNonBlocking, prio_high);
-  if (ce == cudaSuccess)
-    ce = cudaStreamCreateWithFlags(&s->load_large, cudaStreamNonBlocking);
   if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
   s->workers.resize(rc ? 0 : c.workers);
   for (Worker &w : s->workers) {

@@ -575,7 +575,7 @@ typedef struct {
                                 the workers' engines, the batch arenas and a
                                 slab for the relations it holds (the rest,
                                 capped by the device's free memory) */
-  uint32_t workers;          /* concurrent large joins (0: 2) */
+  uint32_t workers;          /* concurrent large joins (0: 1) */
   uint64_t small_tuples;     /* joins below this (|R|+|S|) are batched (0: 4M) */
   uint32_t max_batch_jobs;   /* jobs per batch (0: 256) */
   uint64_t batch_tuples;     /* partition arena of one batch (0: 2^25) */
