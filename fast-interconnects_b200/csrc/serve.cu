@@ -25,7 +25,8 @@
 //  * large joins run on a worker: a resident engine on its own stream,
 //    planned by the autotuner, built once and probed in slices of
 //    probe_slice tuples.  A free worker takes the shortest admitted large
-//    join.  Workers overlap with each other and with batches (one worker by
+//    join (or one that has waited over 0.5 s), and the next one is loaded on
+//    a load stream while the current one runs.  Workers overlap with each other and with batches (one worker by
 //    default: two large joins at once each run at half speed, which only
 //    lengthens their latency).
 //  * completion: the scheduler thread polls the done events, releases the
@@ -69,6 +70,7 @@ struct Request {
   cudaEvent_t ready = nullptr; // relations loaded
   cudaStream_t load = nullptr; // stream that loaded (and frees) them
   bool small = false;
+  bool loaded = false;         // its load is enqueued
   Clock::time_point t_submit, t_admit;
   fi_join_response resp{};
   bool done = false;
@@ -175,6 +177,9 @@ struct fi_join_server {
   void release(Request *r);
   bool dispatch_batches(Clock::time_point now);
   bool dispatch_large();
+  std::deque<Request *>::iterator next_large(Clock::time_point now);
+  Request *prefetched = nullptr;  // last large join loaded ahead of its run
+  cudaStream_t load_large = nullptr;
   bool complete();
   void finish(Request *r, int status);
   void teardown();
@@ -226,6 +231,7 @@ void fi_join_server::release(Request *r) {
 }
 
 void fi_join_server::finish(Request *r, int status) {
+  if (prefetched == r) prefetched = nullptr;
   release(r);
   r->resp.status = status;
   r->resp.latency_us = us_between(r->t_submit, Clock::now());
@@ -245,6 +251,7 @@ void fi_join_server::load(Request *r, cudaStream_t stream) {
   const uint64_t lens[4] = {q.build_len, q.build_len, q.probe_len, q.probe_len};
   const bool host = q.source == FI_SOURCE_HOST;
   cudaStream_t load_stream = stream;
+  r->loaded = true;
   r->load = load_stream;
   const int ncols = host ? 4 : 2;
   unsigned char *at = (unsigned char *)r->block;
@@ -412,14 +419,7 @@ bool fi_join_server::dispatch_large() {
   bool progress = false;
   for (Worker &w : workers) {
     if (w.req || large_q.empty()) continue;
-    // shortest job first among the admitted large joins: a long join no
-    // longer holds up the many shorter ones behind it (arrivals below
-    // capacity bound the wait of the longest)
-    auto pick = large_q.begin();
-    for (auto it = large_q.begin(); it != large_q.end(); ++it)
-      if ((*it)->req.build_len + (*it)->req.probe_len <
-          (*pick)->req.build_len + (*pick)->req.probe_len)
-        pick = it;
+    auto pick = next_large(Clock::now());
     Request *r = *pick;
     large_q.erase(pick);
     progress = true;
@@ -428,7 +428,7 @@ bool fi_join_server::dispatch_large() {
                           "build relation above the server's max_build"));
       continue;
     }
-    load(r, w.stream);
+    if (!r->loaded) load(r, w.stream);
     const int rc = fatal ? fatal : run_large(w, r, cfg.probe_slice);
     if (rc) {
       // the engine may hold work of this request: wait for it before the
@@ -440,7 +440,33 @@ bool fi_join_server::dispatch_large() {
       ++stats.engine_runs;
     }
   }
+  // prefetch: load the next large join while the workers run, so that its
+  // generation or copy overlaps the current join
+  if (!large_q.empty() && !fatal &&
+      (!prefetched || cudaEventQuery(prefetched->ready) != cudaErrorNotReady)) {
+    auto nx = next_large(Clock::now());
+    if (!(*nx)->loaded && (*nx)->req.build_len <= cfg.max_build) {
+      load(*nx, load_large);
+      prefetched = *nx;
+      progress = true;
+    }
+  }
   return progress;
+}
+
+std::deque<Request *>::iterator fi_join_server::next_large(Clock::time_point now) {
+  // shortest job first, so that a long join does not hold up the many
+  // shorter ones behind it; a join that has waited longer than
+  // kMaxLargeWaitUs goes first, which bounds how long the longest wait
+  constexpr double kMaxLargeWaitUs = 500e3;
+  auto pick = large_q.begin();
+  for (auto it = large_q.begin(); it != large_q.end(); ++it) {
+    if (us_between((*it)->t_admit, now) > kMaxLargeWaitUs) return it;
+    if ((*it)->req.build_len + (*it)->req.probe_len <
+        (*pick)->req.build_len + (*pick)->req.probe_len)
+      pick = it;
+  }
+  return pick;
 }
 
 bool fi_join_server::complete() {
@@ -557,11 +583,12 @@ void fi_join_server::teardown() {
     if (r.end) cudaEventDestroy(r.end);
   }
   runners.clear();
-  if (load_small) {
-    cudaStreamSynchronize(load_small);
-    cudaStreamDestroy(load_small);
-    load_small = nullptr;
-  }
+  for (cudaStream_t *ls : {&load_small, &load_large})
+    if (*ls) {
+      cudaStreamSynchronize(*ls);
+      cudaStreamDestroy(*ls);
+      *ls = nullptr;
+    }
   for (auto &kv : all) delete kv.second;
   all.clear();
   if (slab) cudaFree(slab);
@@ -596,6 +623,8 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   cudaError_t ce = cudaStreamCreateWithPriority(&s->load_small,
                                                 cudaStreamNonBlocking, prio_high);
+  if (ce == cudaSuccess)
+    ce = cudaStreamCreateWithFlags(&s->load_large, cudaStreamNonBlocking);
   if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
   s->workers.resize(rc ? 0 : c.workers);
   for (Worker &w : s->workers) {
