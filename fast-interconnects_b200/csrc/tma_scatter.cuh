@@ -9,10 +9,11 @@
 //
 // Measured on B200 (2^28 x 2^28 int64 join, 512 partitions per pass): this
 // path runs the pass-1 scatter at 4.5 TB/s and the pass-2 scatter at 4.1
-// TB/s, against 4.2 and 2.6 TB/s for the register-fed tile scatter.  Two
-// variants with fewer barriers per tile were slower: a two-barrier scan in
-// which every thread sums the warp totals (-16%), and a double-buffered tile
-// histogram cleared during the write-out (-2%).
+// TB/s, against 4.2 and 2.6 TB/s for the register-fed tile scatter.  Slower
+// variants, measured: a two-barrier scan in which every thread sums the warp
+// totals (-16%), a double-buffered tile histogram cleared during the
+// write-out (-2%), two 512-thread CTAs per SM with 2048-tuple tiles (-28%:
+// shorter runs per partition), and TMA bulk stores of the runs (-12%).
 //
 // Requirements checked by the host before choosing this path: 16-byte
 // aligned column/relation bases, tuples of 16 bytes for AoS sources, and a
@@ -59,6 +60,27 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
       : "memory");
 }
 
+// Shared -> global bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned) in this thread's current bulk async-group.
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src,
+                                         uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::
+                   "l"(dst), "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Waits until this thread's committed bulk stores have read their shared
+// memory sources (the buffer may then be overwritten).
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// Waits until this thread's committed bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy (TMA) accesses.
 __device__ __forceinline__ void fence_proxy_async_smem() {
@@ -85,6 +107,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
   return false;
 }
+
+// Write-out of the staged tile by one TMA bulk store per partition run
+// (16-byte tuples: every run starts and ends on a 16-byte boundary) instead
+// of one 16-byte store per tuple by the threads.  Off: measured on B200
+// (1024M x 1024M int64, 9+9 bits) the bulk stores made the pass-1 scatter
+// 8.62 ms instead of 7.59 and the pass-2 scatter 8.71 instead of 8.12; runs
+// average 128 bytes, too short for one bulk copy each to beat the threads'
+// coalesced stores.
+template <typename K>
+constexpr bool kBulkStore = false && sizeof(Tuple<K>) == 16;
 
 template <typename K>
 struct TmaShape {
@@ -198,6 +230,9 @@ __device__ __forceinline__ void tma_tile_scatter_range(
   const uint32_t tid = threadIdx.x;
   if (begin >= end) return;
   const uint64_t ntiles = (end - begin + kTile - 1) / kTile;
+  // bulk stores need 16-byte tuples and a 16-byte aligned output base
+  const bool bulk =
+      kBulkStore<K> && (reinterpret_cast<uintptr_t>(out) % 16) == 0;
 
   if (tid == 0) {
     const uint32_t n0 = (uint32_t)min((uint64_t)kTile, end - begin);
@@ -233,6 +268,7 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     }
     // barrier 1, also the vote on a wait that gave up
     if (__syncthreads_or(!ok)) {
+      if (bulk) bulk_wait_all();
       if (tid == 0) {
         record_error(status, kDevErrTimeout);
         if (t + 1 < ntiles) {  // bounded wait for the copy in flight
@@ -242,22 +278,44 @@ __device__ __forceinline__ void tma_tile_scatter_range(
       }
       return;
     }
+    // the previous tile's bulk stores must have read the staging tile
+    // before anyone stages this one (the scan's barriers order every
+    // thread's wait before the staging writes)
+    if (bulk) bulk_wait_read();
     // 2. run offsets inside the tile
     const uint32_t total = block_exclusive_scan_u32(toff, F, warp_tmp);
     // 3. stage the tile sorted by partition
 #pragma unroll
     for (uint32_t u = 0; u < I; ++u)
       if (u * T + tid < n_valid) staged[toff[pp[u]] + rk[u]] = Tuple<K>{ck[u], cv[u]};
-    __syncthreads();
-    // 4. write the runs: tuple j of run p goes to cur[p] + (j - toff[p])
-    for (uint32_t j = tid; j < n_valid; j += T) {
-      const Tuple<K> tp = staged[j];
-      const uint32_t p = key_to_partition(tp.key, mask, ignore_bits);
-      const uint64_t dst = cur_base + (uint32_t)(cur[p] + (j - toff[p]));
-      if (dst < out_len)
-        store_tuple(out + dst, tp);
-      else
-        record_error(status, kDevErrCapacity);
+    if (bulk) {
+      // 4. one bulk store per partition run, issued by the thread of that
+      // partition once the whole tile is staged
+      fence_proxy_async_smem();
+      __syncthreads();
+      for (uint32_t p = tid; p < F; p += T) {
+        const uint32_t next = (p + 1 < F) ? toff[p + 1] : total;
+        const uint32_t len = next - toff[p];
+        if (len == 0) continue;
+        const uint64_t dst = cur_base + cur[p];
+        if (dst + len <= out_len)
+          bulk_s2g(out + dst, staged + toff[p], len * (uint32_t)sizeof(Tuple<K>));
+        else
+          record_error(status, kDevErrCapacity);
+      }
+      bulk_commit();
+    } else {
+      __syncthreads();
+      // 4. write the runs: tuple j of run p goes to cur[p] + (j - toff[p])
+      for (uint32_t j = tid; j < n_valid; j += T) {
+        const Tuple<K> tp = staged[j];
+        const uint32_t p = key_to_partition(tp.key, mask, ignore_bits);
+        const uint64_t dst = cur_base + (uint32_t)(cur[p] + (j - toff[p]));
+        if (dst < out_len)
+          store_tuple(out + dst, tp);
+        else
+          record_error(status, kDevErrCapacity);
+      }
     }
     __syncthreads();
     // 5. advance the cursors, then clear the tile histogram
@@ -269,6 +327,8 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     for (uint32_t p = tid; p <= F; p += T) toff[p] = 0;
     __syncthreads();
   }
+  // the stores must be complete before the kernel's shared memory goes
+  if (bulk) bulk_wait_all();
 }
 
 }  // namespace fi
