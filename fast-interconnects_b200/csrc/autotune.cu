@@ -12,7 +12,8 @@
 //      shared-memory table each; the 1024M x 1024M int64 join runs fastest
 //      with 2^30 / 2^18), one pass up to 11 bits and two balanced passes
 //      above (a single pass loses its write combining above 11 bits on
-//      B200), bucket chaining, 512-thread join CTAs, TMA-fed scatters.
+//      B200), bucket chaining, 256-thread join CTAs (four per SM), TMA-fed
+//      scatters.
 // Joins below small_tuples in total go to batches.
 #include <cmath>
 #include <cstdio>
@@ -63,7 +64,7 @@ void autotune_model(uint64_t build_len, fi_tuned_plan *out) {
   }
   out->radix_bits.pass_bits[2] = -1;
   out->hashing_scheme = FI_HASHING_BUCKET_CHAINING;
-  out->join_block = 512;
+  out->join_block = 256;
   out->scatter = 0;
 }
 

@@ -18,7 +18,8 @@
 //    bucket-chaining table (u32 heads, u16 next links, keys) sized from the
 //    average build partition, or a perfect-hash array indexed by
 //    key >> ignore_bits.  With blocks of up to 512 threads two CTAs share an
-//    SM, so one CTA's build overlaps the other's probe.  A CTA keeps its
+//    SM (four with up to 256), so one CTA's build overlaps another's probe.
+//    A CTA keeps its
 //    table when its next item belongs to the same partition.  Build values
 //    are not stored: the aggregate only reads s.value.
 //  * A build side larger than the table is joined in rounds (each round
@@ -366,9 +367,14 @@ cudaError_t launch_assign_tasks(const uint64_t *probe_offsets,
 }
 
 template <typename K, int kScheme>
-static const void *join_kernel_ptr(bool two_per_sm) {
-  return two_per_sm ? (const void *)radix_join_kernel<K, kScheme, 512, 2>
-                    : (const void *)radix_join_kernel<K, kScheme, 1024, 1>;
+static const void *join_kernel_ptr(uint32_t ctas_per_sm) {
+  return ctas_per_sm == 4   ? (const void *)radix_join_kernel<K, kScheme, 256, 4>
+         : ctas_per_sm == 2 ? (const void *)radix_join_kernel<K, kScheme, 512, 2>
+                            : (const void *)radix_join_kernel<K, kScheme, 1024, 1>;
+}
+
+uint32_t join_ctas_per_sm(uint32_t block) {
+  return block <= 256 ? 4u : block <= 512 ? 2u : 1u;
 }
 
 template <typename K>
@@ -402,10 +408,11 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
-  // Two CTAs per SM (half the shared memory each) when the block allows it,
-  // so that one CTA's table build overlaps the other's probe.
-  const bool two = block <= 512;
-  const void *fn = scheme == 2 ? join_kernel_ptr<K, 2>(two) : join_kernel_ptr<K, 0>(two);
+  // Several CTAs per SM (an equal share of the shared memory each) when the
+  // block allows it, so that one CTA's table build overlaps another's probe:
+  // 4 CTAs of <= 256 threads, 2 of <= 512, else one of 1024.
+  const uint32_t ctas = join_ctas_per_sm(block);
+  const void *fn = scheme == 2 ? join_kernel_ptr<K, 2>(ctas) : join_kernel_ptr<K, 0>(ctas);
   cudaFuncAttributes attr;
   e = cudaFuncGetAttributes(&attr, fn);
   if (e != cudaSuccess) return e;
@@ -414,9 +421,9 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
   uint32_t dyn = (uint32_t)device_max_smem_optin() - (uint32_t)attr.sharedSizeBytes;
-  if (two) {
-    const int half = per_sm / 2 - reserved - (int)attr.sharedSizeBytes;
-    if (half > 0 && (uint32_t)half < dyn) dyn = (uint32_t)half;
+  if (ctas > 1) {
+    const int share = per_sm / (int)ctas - reserved - (int)attr.sharedSizeBytes;
+    if (share > 0 && (uint32_t)share < dyn) dyn = (uint32_t)share;
   }
   dyn &= ~127u;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
@@ -443,9 +450,13 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
       fanout, ignore_bits, s.item_start, s.item_part, dyn, lb, result_set,     \
       match_count, s.status)
   if (scheme == 2) {
-    if (two) FI_JOIN_LAUNCH(2, 512, 2); else FI_JOIN_LAUNCH(2, 1024, 1);
+    if (ctas == 4) FI_JOIN_LAUNCH(2, 256, 4);
+    else if (ctas == 2) FI_JOIN_LAUNCH(2, 512, 2);
+    else FI_JOIN_LAUNCH(2, 1024, 1);
   } else {
-    if (two) FI_JOIN_LAUNCH(0, 512, 2); else FI_JOIN_LAUNCH(0, 1024, 1);
+    if (ctas == 4) FI_JOIN_LAUNCH(0, 256, 4);
+    else if (ctas == 2) FI_JOIN_LAUNCH(0, 512, 2);
+    else FI_JOIN_LAUNCH(0, 1024, 1);
   }
 #undef FI_JOIN_LAUNCH
   return cudaGetLastError();

@@ -119,6 +119,8 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
                               JoinScratch s, uint32_t sm_count,
                               cudaStream_t stream);
 uint32_t join_items_capacity(uint32_t fanout, uint64_t probe_len);
+// CTAs of `block` threads the join runs per SM (4, 2 or 1).
+uint32_t join_ctas_per_sm(uint32_t block);
 
 // ---- no-partitioning join ------------------------------------------------
 template <typename K>

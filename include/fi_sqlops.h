@@ -368,7 +368,7 @@ uint64_t fi_radix_join_engine_workspace_bytes(const fi_radix_join_engine *e);
  * engine's buffers were sized for the radix bits given at creation; a plan
  * may use fewer bits per pass, one pass instead of two, and tuples no
  * larger than the creation's tuple_bytes.  join_block: threads per join CTA
- * (256, 512 or 1024; 0 = 512).  scatter: 0 = tile scatter fed by TMA bulk
+ * (256: four CTAs per SM, 512: two, 1024: one; 0 = 256).  scatter: 0 = tile scatter fed by TMA bulk
  * copies where the columns allow it, 1 = fed by register loads.  Setting a
  * plan drops a resident build side. */
 typedef struct {
@@ -557,7 +557,7 @@ typedef struct {
  * use the nearest entry of the table loaded by fi_autotune_load (by tuple
  * type, log2 |R|, log2 (|S|/|R|) and skew) or, without one, a model: about
  * 4K build tuples per final partition, one pass up to 11 bits and two
- * balanced passes above, bucket chaining, 512-thread join CTAs, TMA-fed
+ * balanced passes above, bucket chaining, 256-thread join CTAs, TMA-fed
  * scatters.  A table entry may name the perfect scheme, which is valid
  * only for dense unique build keys. */
 int fi_autotune_plan(uint32_t tuple_bytes, uint64_t build_len,
