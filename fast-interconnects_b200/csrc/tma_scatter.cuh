@@ -13,7 +13,11 @@
 // variants, measured: a two-barrier scan in which every thread sums the warp
 // totals (-16%), a double-buffered tile histogram cleared during the
 // write-out (-2%), two 512-thread CTAs per SM with 2048-tuple tiles (-28%:
-// shorter runs per partition), and TMA bulk stores of the runs (-12%).
+// shorter runs per partition), TMA bulk stores of the runs (-12%), and a
+// second pass writing separate key and payload columns so that the join
+// reads build keys only (1024M x 1024M: second-pass scatter 8.1 -> 12.4 ms
+// per relation for a join 0.1 ms faster: each run splits into two runs of
+// half the bytes).
 //
 // Requirements checked by the host before choosing this path: 16-byte
 // aligned column/relation bases, tuples of 16 bytes for AoS sources, and a
