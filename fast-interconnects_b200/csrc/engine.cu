@@ -45,10 +45,18 @@ constexpr uint64_t kPieceTuples = 1ull << 17;
 constexpr uint32_t kChunksPerSm = 1;
 template <typename K>
 using Pass2Shape = TileWide<K>;
-// join launch: four CTAs of 256 threads per SM (measured on B200, 1024M x
-// 1024M int64, 9+9 bits: join 7.48 ms, against 7.78 ms with two CTAs of 512
-// and 9.75 ms with one of 1024)
+// join launch: four CTAs of 256 threads per SM for bucket chaining
+// (measured on B200, 1024M x 1024M int64, 9+9 bits: join 7.48 ms, against
+// 7.78 ms with two CTAs of 512 and 9.75 ms with one of 1024); two CTAs of
+// 512 for the perfect scheme, whose table must span the largest key of a
+// partition: half the SM's shared memory holds ~14.5K int64 keys, the
+// capacity of the reference's one-table-per-CTA sizing
+// (radix-join/src/cuda_radix_join.rs:234-237)
 constexpr uint32_t kJoinBlock = 256;
+constexpr uint32_t kJoinBlockPerfect = 512;
+inline uint32_t default_join_block(fi_hashing_scheme s) {
+  return s == FI_HASHING_PERFECT ? kJoinBlockPerfect : kJoinBlock;
+}
 
 struct Pass2Plan {
   uint64_t *reg_pre;      // [F1][C1+1] prefix of the chunk regions of p1
@@ -403,6 +411,7 @@ extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
   e->bits1 = e->cap1 = b1;
   e->bits2 = e->cap2 = b2;
   e->scheme = hashing_scheme;
+  e->join_block = default_join_block(hashing_scheme);
   e->sm_count = (uint32_t)device_sm_count();
   e->C1 = e->sm_count * kChunksPerSm;
   e->F1 = 1u << b1;
@@ -817,7 +826,8 @@ extern "C" int fi_radix_join_engine_set_plan(fi_radix_join_engine *e,
       plan->hashing_scheme != FI_HASHING_BUCKET_CHAINING)
     return set_error(FI_ERR_UNSUPPORTED,
                      "the radix join supports Perfect and BucketChaining");
-  const uint32_t jb = plan->join_block ? plan->join_block : kJoinBlock;
+  const uint32_t jb =
+      plan->join_block ? plan->join_block : default_join_block(plan->hashing_scheme);
   if (jb != 256 && jb != 512 && jb != 1024)
     return set_error(FI_ERR_INVALID_ARGUMENT, "join_block must be 256, 512 or 1024");
   if (plan->scatter > 1)

@@ -17,7 +17,8 @@
 // second pass writing separate key and payload columns so that the join
 // reads build keys only (1024M x 1024M: second-pass scatter 8.1 -> 12.4 ms
 // per relation for a join 0.1 ms faster: each run splits into two runs of
-// half the bytes).
+// half the bytes), and two barriers fewer per tile (alternating tile
+// histograms, per-run write offsets, one bounds check per run: -4%).
 //
 // Requirements checked by the host before choosing this path: 16-byte
 // aligned column/relation bases, tuples of 16 bytes for AoS sources, and a
