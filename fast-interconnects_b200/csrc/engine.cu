@@ -227,8 +227,8 @@ __global__ void __launch_bounds__(Pass2Shape<K>::kThreads, Pass2Shape<K>::kMinBl
 }
 
 // The same scatter fed by TMA bulk copies of the region segments (16-byte
-// tuples only).  Shared memory: bars | reg_pre | reg_begin | stages |
-// staged tile | toff | cur | scan_tmp.
+// tuples only).  Shared memory: bars | reg_pre | reg_begin | stages | toff |
+// cur | scan_tmp.
 __host__ __device__ inline size_t pass2_tma_tables_bytes(uint32_t C1) {
   return (64 + (2 * (size_t)C1 + 1) * 8 + 127) & ~(size_t)127;
 }
@@ -247,9 +247,8 @@ __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
   uint64_t *reg_pre = bars + 8;             // [C1 + 1]
   uint64_t *reg_begin = reg_pre + C1 + 1;   // [C1]
   unsigned char *stages = smem_raw + pass2_tma_tables_bytes(C1);
-  Tuple<K> *staged =
-      reinterpret_cast<Tuple<K> *>(stages + S::kStages * tma_stage_bytes<K>());
-  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + S::kTile);
+  uint32_t *toff =
+      reinterpret_cast<uint32_t *>(stages + S::kStages * tma_stage_bytes<K>());
   uint32_t *cur = toff + F2 + 1;
   uint32_t *scan_tmp = cur + F2;
   const uint32_t k = blockIdx.x;
@@ -276,7 +275,7 @@ __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
   __syncthreads();
   TmaRegionSource<K> src(rel1, reg_pre, reg_begin, C1);
   tma_tile_scatter_range<K>(src, s0, s1, F2, mask2, ign2, cur, toff, scan_tmp,
-                            staged, stages, bars, rel2, base, rel2_len, status);
+                            stages, bars, rel2, base, rel2_len, status);
 }
 
 template <typename K>

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(S::kThreads, S::kMinBlocks)
 }
 
 // Same as tile_scatter_kernel with TMA-fed input stages (tma_scatter.cuh).
-// Shared memory: bars | stages | staged tile | toff | cur | scan_tmp.
+// Shared memory: bars | stages | toff | cur | scan_tmp.
 template <typename K>
 __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
     tma_tile_scatter_kernel(const K *__restrict__ keys,
@@ -80,9 +80,8 @@ __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
   const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
   unsigned char *stages = smem_raw + 64;
-  Tuple<K> *staged =
-      reinterpret_cast<Tuple<K> *>(stages + S::kStages * tma_stage_bytes<K>());
-  uint32_t *toff = reinterpret_cast<uint32_t *>(staged + S::kTile);
+  uint32_t *toff =
+      reinterpret_cast<uint32_t *>(stages + S::kStages * tma_stage_bytes<K>());
   uint32_t *cur = toff + F + 1;
   uint32_t *scan_tmp = cur + F;
 
@@ -99,7 +98,7 @@ __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
   __syncthreads();
   TmaColumnSource<K> src{keys, pays};
   tma_tile_scatter_range<K>(src, cb, ce, F, mask, ignore_bits, cur, toff,
-                            scan_tmp, staged, stages, bars, out, base, out_len,
+                            scan_tmp, stages, bars, out, base, out_len,
                             status);
 }
 

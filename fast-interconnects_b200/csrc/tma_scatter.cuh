@@ -7,22 +7,31 @@
 // instead of 16) to hide the shared-memory latency of ranking and staging,
 // and the loads of tile t+1 stay in flight for the whole of tile t.
 //
-// Measured on B200 (2^28 x 2^28 int64 join, 512 partitions per pass): this
-// path runs the pass-1 scatter at 4.5 TB/s and the pass-2 scatter at 4.1
-// TB/s, against 4.2 and 2.6 TB/s for the register-fed tile scatter.  Slower
+// Each tile is sorted in place in its own stage (tuples held in registers
+// across the scan), so two stages of 6144 int64 tuples fit where two stages
+// plus a separate staging tile of 4096 did.  Measured on B200 (1024M x 1024M
+// int64 join, 9+9 bits): pass-1 scatter 7.59 -> 6.96 ms and pass-2 scatter
+// 8.13 -> 7.38 ms per relation against the 4096-tuple tiles with a staging
+// tile; 7040-tuple tiles (the shared-memory limit) gave 6.92 ms.  Slower
 // variants, measured: a two-barrier scan in which every thread sums the warp
 // totals (-16%), a double-buffered tile histogram cleared during the
 // write-out (-2%), two 512-thread CTAs per SM with 2048-tuple tiles (-28%:
-// shorter runs per partition), TMA bulk stores of the runs (-12%), and a
-// second pass writing separate key and payload columns so that the join
-// reads build keys only (1024M x 1024M: second-pass scatter 8.1 -> 12.4 ms
-// per relation for a join 0.1 ms faster: each run splits into two runs of
-// half the bytes), and two barriers fewer per tile (alternating tile
-// histograms, per-run write offsets, one bounds check per run: -4%).
+// shorter runs per partition), TMA bulk stores of the runs (-12%), a second
+// pass writing separate key and payload columns so that the join reads
+// build keys only (second-pass scatter 8.1 -> 12.4 ms per relation for a
+// join 0.1 ms faster: each run splits into two runs of half the bytes), two
+// barriers fewer per tile (alternating tile histograms, per-run write
+// offsets, one bounds check per run: -4%), and warp specialisation (16
+// warps ranking and sorting tile t+1 while 16 write out tile t, three
+// 4096-tuple buffers handed over by mbarriers: 7.58 and 7.81 ms, no gain:
+// the sorting work, not the serialisation of the phases, bounds the SM).
+// An ablation on 2^30 int64 tuples (9 bits, 4096-tuple tiles) located the
+// time: without the global stores 6.1 of 7.6 ms remain, without the
+// write-out loop 5.1, without the staging 3.9.
 //
 // Requirements checked by the host before choosing this path: 16-byte
 // aligned column/relation bases, tuples of 16 bytes for AoS sources, and a
-// fanout small enough that two stages + the staging tile fit shared memory.
+// fanout small enough that the two stages fit shared memory.
 // Every mbarrier wait is bounded; a wait that gives up records
 // kDevErrTimeout, waits (bounded) for the copy it issued and returns.
 #pragma once
@@ -65,27 +74,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
       : "memory");
 }
 
-// Shared -> global bulk copy of `bytes` (multiple of 16, both addresses
-// 16-byte aligned) in this thread's current bulk async-group.
-__device__ __forceinline__ void bulk_s2g(void *dst, const void *src,
-                                         uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::
-                   "l"(dst), "r"(smem_u32(src)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() {
-  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-// Waits until this thread's committed bulk stores have read their shared
-// memory sources (the buffer may then be overwritten).
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-// Waits until this thread's committed bulk stores are complete.
-__device__ __forceinline__ void bulk_wait_all() {
-  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-}
-
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy (TMA) accesses.
 __device__ __forceinline__ void fence_proxy_async_smem() {
@@ -113,20 +101,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
-// Write-out of the staged tile by one TMA bulk store per partition run
-// (16-byte tuples: every run starts and ends on a 16-byte boundary) instead
-// of one 16-byte store per tuple by the threads.  Off: measured on B200
-// (1024M x 1024M int64, 9+9 bits) the bulk stores made the pass-1 scatter
-// 8.62 ms instead of 7.59 and the pass-2 scatter 8.71 instead of 8.12; runs
-// average 128 bytes, too short for one bulk copy each to beat the threads'
-// coalesced stores.
-template <typename K>
-constexpr bool kBulkStore = false && sizeof(Tuple<K>) == 16;
 
 template <typename K>
 struct TmaShape {
   static constexpr uint32_t kThreads = 1024;
-  static constexpr uint32_t kItems = sizeof(K) == 8 ? 4 : 8;
+  static constexpr uint32_t kItems = sizeof(K) == 8 ? 6 : 12;
   static constexpr uint32_t kTile = kThreads * kItems;
   static constexpr uint32_t kStages = 2;
 };
@@ -137,12 +116,11 @@ constexpr size_t tma_stage_bytes() {
   return (size_t)TmaShape<K>::kTile * 2 * sizeof(K);
 }
 
-// Shared memory: [bars (64 B)] [stages] [staged tile]
-//                [toff F+1] [cur F] [warp_tmp 33]
+// Shared memory: [bars (64 B)] [stages] [toff F+1] [cur F] [warp_tmp 33]
+// (a tile is sorted in place in its own stage)
 template <typename K>
 size_t tma_scatter_smem(uint32_t F) {
   return 64 + TmaShape<K>::kStages * tma_stage_bytes<K>() +
-         (size_t)TmaShape<K>::kTile * sizeof(Tuple<K>) +
          (size_t)(2 * F + 1 + 33) * sizeof(uint32_t);
 }
 
@@ -218,26 +196,25 @@ struct TmaRegionSource {
 // Scatters logical src[begin, end) by partition: partition p's tuples go to
 // out[cur_base + cur[p]], out[cur_base + cur[p] + 1], ...  Shared memory:
 // `cur` (F u32, relative to cur_base), `toff` (tile histogram, F+1 u32, zero
-// on entry and exit), `warp_tmp` (33 u32), `staged` (kTile tuples), `stages`
-// (kStages input stages) and `bars` (one mbarrier per stage, initialised
-// with count 1).  Called once per barrier initialisation by all threads;
-// thread 0 issues the copies.
+// on entry and exit), `warp_tmp` (33 u32), `stages` (kStages input stages)
+// and `bars` (one mbarrier per stage, initialised with count 1).  A tile is
+// sorted in place: every thread holds its tuples in registers across the
+// scan, then writes them back into the tile's own stage in partition order,
+// so no separate staging buffer is needed and the stages can be 50% longer.
+// Called once per barrier initialisation by all threads; thread 0 issues
+// the copies.
 template <typename K, typename Src>
 __device__ __forceinline__ void tma_tile_scatter_range(
     Src &src, uint64_t begin, uint64_t end, uint32_t F, uint64_t mask,
     uint32_t ignore_bits, uint32_t *cur, uint32_t *toff, uint32_t *warp_tmp,
-    Tuple<K> *staged, unsigned char *stages, uint64_t *bars,
-    Tuple<K> *__restrict__ out, uint64_t cur_base, uint64_t out_len,
-    int *status) {
+    unsigned char *stages, uint64_t *bars, Tuple<K> *__restrict__ out,
+    uint64_t cur_base, uint64_t out_len, int *status) {
   using S = TmaShape<K>;
   constexpr uint32_t T = S::kThreads, I = S::kItems, kTile = S::kTile;
   constexpr size_t kStageBytes = tma_stage_bytes<K>();
   const uint32_t tid = threadIdx.x;
   if (begin >= end) return;
   const uint64_t ntiles = (end - begin + kTile - 1) / kTile;
-  // bulk stores need 16-byte tuples and a 16-byte aligned output base
-  const bool bulk =
-      kBulkStore<K> && (reinterpret_cast<uintptr_t>(out) % 16) == 0;
 
   if (tid == 0) {
     const uint32_t n0 = (uint32_t)min((uint64_t)kTile, end - begin);
@@ -248,8 +225,8 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     const uint32_t parity = (uint32_t)((t / S::kStages) & 1u);
     const uint64_t t0 = begin + t * kTile;
     const uint32_t n_valid = (uint32_t)min((uint64_t)kTile, end - t0);
-    // prefetch the next tile into the other stage; its previous contents
-    // (tile t-1) were consumed before the last barrier of tile t-1
+    // prefetch the next tile into the other stage; tile t-1 finished with it
+    // (every thread fenced its accesses before the last barrier of t-1)
     if (tid == 0 && t + 1 < ntiles) {
       const uint64_t t1 = t0 + kTile;
       const uint32_t s1 = (uint32_t)((t + 1) % S::kStages);
@@ -258,7 +235,7 @@ __device__ __forceinline__ void tma_tile_scatter_range(
                 stages + s1 * kStageBytes, &bars[s1]);
     }
     const bool ok = mbar_wait(&bars[s], parity);
-    const unsigned char *stage = stages + s * kStageBytes;
+    unsigned char *stage = stages + s * kStageBytes;
 
     // 1. rank every tuple inside its partition's run of the tile
     K ck[I], cv[I];
@@ -271,9 +248,9 @@ __device__ __forceinline__ void tma_tile_scatter_range(
       pp[u] = act ? key_to_partition(ck[u], mask, ignore_bits) : 0u;
       rk[u] = warp_aggregated_rank(toff, pp[u], act);
     }
-    // barrier 1, also the vote on a wait that gave up
+    // barrier 1: every tuple of the stage is in registers; also the vote on
+    // a wait that gave up
     if (__syncthreads_or(!ok)) {
-      if (bulk) bulk_wait_all();
       if (tid == 0) {
         record_error(status, kDevErrTimeout);
         if (t + 1 < ntiles) {  // bounded wait for the copy in flight
@@ -283,57 +260,35 @@ __device__ __forceinline__ void tma_tile_scatter_range(
       }
       return;
     }
-    // the previous tile's bulk stores must have read the staging tile
-    // before anyone stages this one (the scan's barriers order every
-    // thread's wait before the staging writes)
-    if (bulk) bulk_wait_read();
     // 2. run offsets inside the tile
-    const uint32_t total = block_exclusive_scan_u32(toff, F, warp_tmp);
-    // 3. stage the tile sorted by partition
+    block_exclusive_scan_u32(toff, F, warp_tmp);
+    // 3. write the tile back into its stage, sorted by partition
+    Tuple<K> *staged = reinterpret_cast<Tuple<K> *>(stage);
 #pragma unroll
     for (uint32_t u = 0; u < I; ++u)
       if (u * T + tid < n_valid) staged[toff[pp[u]] + rk[u]] = Tuple<K>{ck[u], cv[u]};
-    if (bulk) {
-      // 4. one bulk store per partition run, issued by the thread of that
-      // partition once the whole tile is staged
-      fence_proxy_async_smem();
-      __syncthreads();
-      for (uint32_t p = tid; p < F; p += T) {
-        const uint32_t next = (p + 1 < F) ? toff[p + 1] : total;
-        const uint32_t len = next - toff[p];
-        if (len == 0) continue;
-        const uint64_t dst = cur_base + cur[p];
-        if (dst + len <= out_len)
-          bulk_s2g(out + dst, staged + toff[p], len * (uint32_t)sizeof(Tuple<K>));
-        else
-          record_error(status, kDevErrCapacity);
-      }
-      bulk_commit();
-    } else {
-      __syncthreads();
-      // 4. write the runs: tuple j of run p goes to cur[p] + (j - toff[p])
-      for (uint32_t j = tid; j < n_valid; j += T) {
-        const Tuple<K> tp = staged[j];
-        const uint32_t p = key_to_partition(tp.key, mask, ignore_bits);
-        const uint64_t dst = cur_base + (uint32_t)(cur[p] + (j - toff[p]));
-        if (dst < out_len)
-          store_tuple(out + dst, tp);
-        else
-          record_error(status, kDevErrCapacity);
-      }
+    __syncthreads();
+    // 4. write the runs: tuple j of run p goes to cur[p] + (j - toff[p])
+    for (uint32_t j = tid; j < n_valid; j += T) {
+      const Tuple<K> tp = staged[j];
+      const uint32_t p = key_to_partition(tp.key, mask, ignore_bits);
+      const uint64_t dst = cur_base + (uint32_t)(cur[p] + (j - toff[p]));
+      if (dst < out_len)
+        store_tuple(out + dst, tp);
+      else
+        record_error(status, kDevErrCapacity);
     }
+    fence_proxy_async_smem();  // this stage's generic accesses before its refill
     __syncthreads();
     // 5. advance the cursors, then clear the tile histogram
     for (uint32_t p = tid; p < F; p += T) {
-      const uint32_t next = (p + 1 < F) ? toff[p + 1] : total;
+      const uint32_t next = (p + 1 < F) ? toff[p + 1] : n_valid;
       cur[p] += next - toff[p];
     }
     __syncthreads();
     for (uint32_t p = tid; p <= F; p += T) toff[p] = 0;
     __syncthreads();
   }
-  // the stores must be complete before the kernel's shared memory goes
-  if (bulk) bulk_wait_all();
 }
 
 }  // namespace fi
