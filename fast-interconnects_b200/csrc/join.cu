@@ -30,6 +30,14 @@
 //  * Each thread adds its sum into result_set[global thread] (the reference's
 //    output convention, cuda_radix_join.rs:15-30); match counts are reduced
 //    per CTA and added to one u64.
+//  * Measured on B200 and left out (1024M x 1024M int64, 9+9 bits, join 7.47
+//    ms with four 256-thread CTAs per SM): a TMA-fed variant (one 1024-thread
+//    CTA per SM, the next item's build side bulk-copied into a staging buffer
+//    while the current item probes, probe tuples in two 2048-tuple chunk
+//    buffers): 9.63 ms, since 227 KB cannot keep a whole next partition in
+//    flight and each item waits on its first chunks; bulk L2 prefetches of
+//    the next item's build and probe ranges: 10.37 ms; eight probe loads in
+//    flight per thread instead of four: 9.16 ms (register spills).
 #include "common.cuh"
 #include "kernels.h"
 
