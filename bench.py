@@ -55,10 +55,20 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
-                    choices=["join", "partition", "ooc", "serve"],
+                    choices=["join", "partition", "ooc", "serve", "dataset"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
-                         "join server against back-to-back plain calls")
+                         "join server against back-to-back plain calls; dataset: "
+                         "a named data set of the reference (--data-set)")
+    ap.add_argument("--data-set", default="blanas",
+                    choices=["blanas", "blanas4mb", "kim", "lutz2gv32g", "lutz32gv32g"],
+                    help="dataset workload: Blanas 16M x 256M int64, Kim 128e6 x "
+                         "128e6 int32 (the papers' key sizes), ...")
+    ap.add_argument("--tuple-bytes", type=int, default=0,
+                    help="dataset workload: 8 (int32) or 16 (int64); 0 = the "
+                         "data set's own")
+    ap.add_argument("--selectivity", type=int, default=100,
+                    help="dataset workload: join selectivity in percent")
     ap.add_argument("--ooc-log2n", type=int, default=31,
                     help="out-of-core join: |R| = |S| = 2^ooc_log2n int64 tuples")
     ap.add_argument("--ooc-block", type=int, default=0,
@@ -858,6 +868,113 @@ def run_serve(a):
         dist.destroy_process_group()
 
 
+DATASETS = {  # name -> (fi.Dataset member, tuple bytes of the paper)
+    "blanas": ("Blanas", 16), "blanas4mb": ("Blanas4MB", 16), "kim": ("Kim", 8),
+    "lutz2gv32g": ("Lutz2Gv32G", 16), "lutz32gv32g": ("Lutz32Gv32G", 16)}
+
+
+def run_dataset(a):
+    """Join of one of the reference's named data sets (seeded primary keys
+    with the join selectivity applied, uniform foreign keys, payload = key)
+    on the autotuner's plan; checked against the match count and payload sum
+    recomputed from the selectivity draw of each foreign key."""
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    name, paper_tb = DATASETS[a.data_set]
+    tb = a.tuple_bytes or paper_tb
+    dt = torch.int32 if tb == 8 else torch.int64
+    ds = getattr(fi.Dataset, name)
+    seed = a.seed + 1000 * rank
+    rk, rp, sk, sp = fi.gen_dataset(ds, dt, selectivity=a.selectivity, seed=seed)
+    nb, npr = rk.numel(), sk.numel()
+    kept = fi.null_keys(sk.clone(), a.selectivity, seed + 7) != -1
+    exp_c = int(kept.sum().item())
+    exp_s = int(sp.to(torch.int64)[kept].sum().item())
+    del kept
+    plan = fi.autotune_plan(tb, nb, npr, small_tuples=1)
+    bits = plan["bits"] if plan["bits"] and plan["bits"][0] > 0 else (1,)
+    engine = fi.RadixJoinEngine(nb, npr, dt, fi.RadixBits(*bits),
+                                fi.HashingScheme.BucketChaining)
+    engine.set_plan(fi.RadixBits(*bits), fi.HashingScheme.BucketChaining,
+                    plan["join_block"], plan["scatter"])
+    stream = torch.cuda.current_stream()
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        s, c = engine.run(rk, rp, sk, sp)
+        verified = verified and (s, c) == (exp_s, exp_c)
+    engine.status()
+    K = a.steps
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(K):
+            engine.run_async(rk, rp, sk, sp)
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    r = engine.result.cpu()
+    verified = verified and (int(r[0]), int(r[1])) == (exp_s, exp_c)
+    ms = max_over_ranks(start.elapsed_time(end), world) / K
+    value = world * (nb + npr) / (ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    kb = tb // 2
+    pipe_bytes = (nb + npr) * (kb + len(bits) * 2 * tb + tb)
+    e2e = None
+    if not a.no_e2e and a.e2e_steps > 0:
+        host = [torch.empty(x.numel(), dtype=dt, pin_memory=True) for x in (rk, rp, sk, sp)]
+        for h, d in zip(host, (rk, rp, sk, sp)):
+            h.copy_(d)
+        del rk, rp, sk, sp
+        torch.cuda.empty_cache()
+        engine.run_host(*host)
+        t_e2e = []
+        for _ in range(a.e2e_steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            s, c = engine.run_host(*host)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            verified = verified and (s, c) == (exp_s, exp_c)
+            t_e2e.append(t0.elapsed_time(t1))
+        e2e_ms = max_over_ranks(statistics.mean(t_e2e), world)
+        e2e = {"value": world * (nb + npr) / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 2 * (nb + npr) * kb, "d2h_bytes_per_step": 16,
+               "ms_per_step": e2e_ms,
+               "path": "fi_radix_join_engine_run_host_%s (pinned host columns)"
+                       % ("int32" if tb == 8 else "int64")}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": K, "warmup": a.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int32" if tb == 8 else "int64",
+                "data": "synthetic %s data set (seeded permutation PK with %d%% "
+                        "selectivity, uniform FK, payload = key)" % (name, a.selectivity),
+                "config": {"workload": "radix_join_%s_%s_sel%d" % (
+                               a.data_set, "int32" if tb == 8 else "int64", a.selectivity),
+                           "build_tuples": nb, "probe_tuples": npr,
+                           "radix_bits": list(bits), "hashing_scheme": "chaining",
+                           "join_block": plan["join_block"],
+                           "l2_flush": "none: inputs larger than L2" if (nb + npr) * tb > 2**27
+                                       else "none: inputs smaller than L2",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "pipeline_roofline": {"algorithmic_bytes_per_step": pipe_bytes,
+                                      "achieved_gb_per_s": pipe_bytes / (ms / 1e3) / 1e9,
+                                      "frac_of_peak": pipe_bytes / (ms / 1e3) / 1e9 / peak,
+                                      "peak": peak, "peak_source": peak_kind},
+                "e2e": e2e, "gpu_launches": engine.last_launches() * K,
+                "clocks": clk.summary(), "matches": exp_c,
+                "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -868,6 +985,8 @@ def main():
         run_ooc(a)
     elif a.workload == "serve":
         run_serve(a)
+    elif a.workload == "dataset":
+        run_dataset(a)
     else:
         run_ours(a)
 

@@ -961,3 +961,55 @@ extern "C" int fi_datagen_uniform_u64_keys(int64_t *keys, uint64_t n,
                                            uint64_t seed, fi_stream_t stream) {
   FI_GEN_RC(launch_gen_uniform_u64(keys, n, seed, (cudaStream_t)stream));
 }
+extern "C" int fi_datagen_null_keys_int32(int32_t *keys, uint64_t n,
+                                          uint32_t selectivity, uint64_t seed,
+                                          int32_t base, fi_stream_t stream) {
+  if (selectivity > 100)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "selectivity is a percentage");
+  FI_GEN_RC(launch_null_keys<int32_t>(keys, n, selectivity, seed, base,
+                                      (cudaStream_t)stream));
+}
+extern "C" int fi_datagen_null_keys_int64(int64_t *keys, uint64_t n,
+                                          uint32_t selectivity, uint64_t seed,
+                                          int64_t base, fi_stream_t stream) {
+  if (selectivity > 100)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "selectivity is a percentage");
+  FI_GEN_RC(launch_null_keys<int64_t>(keys, n, selectivity, seed, base,
+                                      (cudaStream_t)stream));
+}
+
+// Data set shapes (datagen/src/popular.rs:22-105 and the data sets of
+// radix-join/src/main.rs:657-760).
+extern "C" int fi_dataset_shape(fi_dataset d, uint32_t tuple_bytes,
+                                uint64_t *build_len, uint64_t *probe_len) {
+  if (!build_len || !probe_len) return set_error(FI_ERR_INVALID_ARGUMENT, "null output");
+  if (tuple_bytes != 8 && tuple_bytes != 16)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "tuple_bytes must be 8 or 16");
+  switch (d) {
+    case FI_DATASET_BLANAS:
+      *build_len = 16ull << 20;
+      *probe_len = 256ull << 20;
+      return FI_OK;
+    case FI_DATASET_BLANAS4MB:
+      *build_len = 512ull << 10;
+      *probe_len = 256ull << 20;
+      return FI_OK;
+    case FI_DATASET_KIM:
+      *build_len = 128000000ull;
+      *probe_len = 128000000ull;
+      return FI_OK;
+    case FI_DATASET_TEST:
+      *build_len = 1000;
+      *probe_len = 1000;
+      return FI_OK;
+    case FI_DATASET_LUTZ2GV32G:
+      *build_len = (2ull << 30) / tuple_bytes;
+      *probe_len = (32ull << 30) / tuple_bytes;
+      return FI_OK;
+    case FI_DATASET_LUTZ32GV32G:
+      *build_len = (32ull << 30) / tuple_bytes;
+      *probe_len = (32ull << 30) / tuple_bytes;
+      return FI_OK;
+  }
+  return set_error(FI_ERR_INVALID_ARGUMENT, "unknown data set %d", (int)d);
+}

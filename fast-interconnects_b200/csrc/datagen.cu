@@ -133,6 +133,27 @@ __global__ void gen_u64_kernel(int64_t *keys, uint64_t n, uint64_t seed) {
     keys[i] = (int64_t)dg_mix64(seed ^ dg_mix64(i + 0x1234567ull));
 }
 
+// Join selectivity (datagen/src/relation.rs:85-151): the reference keeps a
+// primary key when a uniform draw from 0..=100 is at most `selectivity` and
+// otherwise stores the null key.  Here the draw is a function of (seed,
+// key - base), so a caller can recompute from a key alone whether it stayed.
+__host__ __device__ __forceinline__ bool dg_keep_key(uint64_t seed, uint64_t off,
+                                                     uint32_t selectivity) {
+  return dg_mix64(seed ^ dg_mix64(off + 0x6E756C6Cull)) % 101u <= selectivity;
+}
+
+template <typename K>
+__global__ void null_keys_kernel(K *keys, uint64_t n, uint32_t selectivity,
+                                 uint64_t seed, K base) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    if (k == null_key<K>()) continue;
+    const uint64_t off = (uint64_t)((int64_t)k - (int64_t)base);
+    if (!dg_keep_key(seed, off, selectivity)) keys[i] = null_key<K>();
+  }
+}
+
 static uint32_t gen_grid(uint64_t n) {
   uint64_t g = (n + 255) / 256;
   return (uint32_t)(g < 148u * 64u ? (g == 0 ? 1 : g) : 148u * 64u);
@@ -165,6 +186,19 @@ cudaError_t launch_gen_zipf_fk(K *keys, uint64_t n, uint64_t pk_n, double s,
       keys, n, pk_n, s, seed, make_perm(pk_n, pk_seed), base);
   return cudaGetLastError();
 }
+
+template <typename K>
+cudaError_t launch_null_keys(K *keys, uint64_t n, uint32_t selectivity,
+                             uint64_t seed, K base, cudaStream_t stream) {
+  if (n == 0 || selectivity >= 100) return cudaSuccess;
+  null_keys_kernel<K><<<gen_grid(n), 256, 0, stream>>>(keys, n, selectivity, seed,
+                                                       base);
+  return cudaGetLastError();
+}
+template cudaError_t launch_null_keys<int32_t>(int32_t *, uint64_t, uint32_t,
+                                               uint64_t, int32_t, cudaStream_t);
+template cudaError_t launch_null_keys<int64_t>(int64_t *, uint64_t, uint32_t,
+                                               uint64_t, int64_t, cudaStream_t);
 
 cudaError_t launch_gen_uniform_u64(int64_t *keys, uint64_t n, uint64_t seed,
                                    cudaStream_t stream) {

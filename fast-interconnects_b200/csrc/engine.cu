@@ -751,29 +751,29 @@ extern "C" int fi_radix_join_engine_run_int64(
                              probe_pay, probe_len, result, (cudaStream_t)stream);
 }
 
-extern "C" int fi_radix_join_engine_run_host_int64(
-    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
-    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
-    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+template <typename K>
+static int engine_run_host(fi_radix_join_engine *e, const K *build_key,
+                           const K *build_pay, uint64_t build_len,
+                           const K *probe_key, const K *probe_pay,
+                           uint64_t probe_len, fi_join_result *result,
+                           cudaStream_t st) {
   if (!e || !result) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
-  cudaStream_t st = (cudaStream_t)stream;
-  const int64_t *src[4] = {build_key, build_pay, probe_key, probe_pay};
+  const K *src[4] = {build_key, build_pay, probe_key, probe_pay};
   const uint64_t lens[4] = {build_len, build_len, probe_len, probe_len};
   for (int i = 0; i < 4; ++i) {
-    int rc = e->in_cols[i].reserve(std::max<uint64_t>(lens[i], 1) * 8, false);
+    int rc = e->in_cols[i].reserve(std::max<uint64_t>(lens[i], 1) * sizeof(K), false);
     if (rc) return rc;
-    FI_CK(cudaMemcpyAsync(e->in_cols[i].ptr, src[i], lens[i] * 8,
+    FI_CK(cudaMemcpyAsync(e->in_cols[i].ptr, src[i], lens[i] * sizeof(K),
                           cudaMemcpyHostToDevice, st),
           "host-to-device copy");
   }
   DevBuf dres;
   int rc = dres.reserve(sizeof(fi_join_result), false);
   if (rc) return rc;
-  rc = engine_run<int64_t>(e, (const int64_t *)e->in_cols[0].ptr,
-                           (const int64_t *)e->in_cols[1].ptr, build_len,
-                           (const int64_t *)e->in_cols[2].ptr,
-                           (const int64_t *)e->in_cols[3].ptr, probe_len,
-                           (fi_join_result *)dres.ptr, st);
+  rc = engine_run<K>(e, (const K *)e->in_cols[0].ptr, (const K *)e->in_cols[1].ptr,
+                     build_len, (const K *)e->in_cols[2].ptr,
+                     (const K *)e->in_cols[3].ptr, probe_len,
+                     (fi_join_result *)dres.ptr, st);
   if (rc == FI_OK) {
     cudaError_t ce = cudaMemcpyAsync(result, dres.ptr, sizeof(fi_join_result),
                                      cudaMemcpyDeviceToHost, st);
@@ -782,6 +782,21 @@ extern "C" int fi_radix_join_engine_run_host_int64(
   }
   dres.release();
   return rc;
+}
+
+extern "C" int fi_radix_join_engine_run_host_int32(
+    fi_radix_join_engine *e, const int32_t *build_key, const int32_t *build_pay,
+    uint64_t build_len, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_run_host<int32_t>(e, build_key, build_pay, build_len, probe_key,
+                                  probe_pay, probe_len, result, (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_run_host_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, fi_join_result *result, fi_stream_t stream) {
+  return engine_run_host<int64_t>(e, build_key, build_pay, build_len, probe_key,
+                                  probe_pay, probe_len, result, (cudaStream_t)stream);
 }
 
 extern "C" int fi_radix_join_engine_build_int32(fi_radix_join_engine *e,

@@ -147,6 +147,9 @@ template <typename K>
 cudaError_t launch_gen_zipf_fk(K *keys, uint64_t n, uint64_t pk_n, double s,
                                uint64_t seed, uint64_t pk_seed, K base,
                                cudaStream_t stream);
+template <typename K>
+cudaError_t launch_null_keys(K *keys, uint64_t n, uint32_t selectivity,
+                             uint64_t seed, K base, cudaStream_t stream);
 cudaError_t launch_gen_uniform_u64(int64_t *keys, uint64_t n, uint64_t seed,
                                    cudaStream_t stream);
 

@@ -511,9 +511,10 @@ class RadixJoinEngine:
         return int(r[0]), int(r[1]) & ((1 << 64) - 1)
 
     def run_host(self, build_key, build_pay, probe_key, probe_pay, stream=None):
-        """Host (pinned) int64 columns in, (sum, count) out; synchronous."""
+        """Host (pinned) columns in, (sum, count) out; synchronous."""
         res = _JoinResultC()
-        _check(lib().fi_radix_join_engine_run_host_int64(
+        f = getattr(lib(), "fi_radix_join_engine_run_host_" + _sfx(build_key.dtype))
+        _check(f(
             self.h, _ptr(build_key), _ptr(build_pay),
             C.c_uint64(build_key.numel()), _ptr(probe_key), _ptr(probe_pay),
             C.c_uint64(probe_key.numel()), C.byref(res), _stream(stream)))
@@ -756,3 +757,80 @@ def gen_uniform_u64_keys(t, seed, stream=None):
     _check(lib().fi_datagen_uniform_u64_keys(_ptr(t), C.c_uint64(t.numel()),
                                              C.c_uint64(seed), _stream(stream)))
     return t
+
+
+def null_keys(t, selectivity, seed, base=1, stream=None):
+    """Join selectivity in percent (fi_datagen_null_keys): each key of `t`
+    stays with probability (selectivity+1)/101, a function of (seed, key -
+    base), and becomes the null key (-1) otherwise; selectivity 100 keeps
+    all keys.  Apply it to primary keys base..base+n-1."""
+    f = getattr(lib(), "fi_datagen_null_keys_" + _sfx(t.dtype))
+    _check(f(_ptr(t), C.c_uint64(t.numel()), C.c_uint32(selectivity),
+             C.c_uint64(seed), _ctype(t.dtype)(base), _stream(stream)))
+    return t
+
+
+# ---------------------------------------------------------------------------
+# data sets and relation files
+# ---------------------------------------------------------------------------
+class Dataset(enum.IntEnum):
+    """The reference's named data sets (radix-join/src/main.rs:657-760)."""
+    Blanas = 0
+    Blanas4MB = 1
+    Kim = 2
+    Test = 3
+    Lutz2Gv32G = 4
+    Lutz32Gv32G = 5
+
+
+def dataset_shape(dataset, dtype):
+    """(|R|, |S|) of a named data set for tuples of two `dtype` values."""
+    b, p = C.c_uint64(), C.c_uint64()
+    _check(lib().fi_dataset_shape(int(dataset), _tuple_bytes(dtype), C.byref(b),
+                                  C.byref(p)))
+    return b.value, p.value
+
+
+def gen_dataset(dataset, dtype, selectivity=100, seed=0, stream=None):
+    """Device columns (build_key, build_pay, probe_key, probe_pay) of a named
+    data set: primary keys a seeded permutation of 1..|R| with
+    (100 - selectivity)% nulled, foreign keys uniform over 1..|R|, payload =
+    key (the reference leaves the payload columns unset for these sets)."""
+    nb, npr = dataset_shape(dataset, dtype)
+    rk = torch.empty(nb, dtype=dtype, device="cuda")
+    sk = torch.empty(npr, dtype=dtype, device="cuda")
+    gen_primary_keys(rk, seed, base=1, stream=stream)
+    null_keys(rk, selectivity, seed + 7, base=1, stream=stream)
+    gen_uniform_foreign_keys(sk, nb, seed + 1, base=1, stream=stream)
+    return rk, rk.clone(), sk, sk.clone()
+
+
+def relation_file_len(path):
+    """Tuples in a relation file (fi_relation_file_len)."""
+    n = C.c_uint64()
+    _check(lib().fi_relation_file_len(os.fsencode(path), C.byref(n)))
+    return n.value
+
+
+def read_relation_file(path, dtype=torch.int64, pin=None):
+    """(keys, payloads) of a relation file as host tensors, pinned when a GPU
+    is present (pin=None) so that the engine's host entry points copy them
+    directly."""
+    if pin is None:
+        pin = torch.cuda.is_available()
+    n = relation_file_len(path)
+    keys = torch.empty(n, dtype=dtype, pin_memory=pin)
+    pays = torch.empty(n, dtype=dtype, pin_memory=pin)
+    f = getattr(lib(), "fi_relation_file_read_" + _sfx(dtype))
+    _check(f(os.fsencode(path), C.c_void_p(keys.data_ptr() if n else 0),
+             C.c_void_p(pays.data_ptr() if n else 0), C.c_uint64(n)))
+    return keys, pays
+
+
+def load_join_data(inner_path, outer_path, dtype=torch.int64, pin=None):
+    """build_with_files (data-store/src/join_data.rs:173-280): the inner
+    (build) and outer (probe) relations as host columns (build_key,
+    build_pay, probe_key, probe_pay)."""
+    rk, rp = read_relation_file(inner_path, dtype, pin)
+    sk, sp = read_relation_file(outer_path, dtype, pin)
+    return rk, rp, sk, sp

@@ -453,6 +453,15 @@ int fi_radix_join_engine_run_int64(fi_radix_join_engine *e,
 /* Same join from host memory (ideally pinned): copies the four columns to
  * the device inside the call, runs the join and copies the result back into
  * the host `result`.  Synchronous. */
+int fi_radix_join_engine_run_host_int32(fi_radix_join_engine *e,
+                                        const int32_t *build_key,
+                                        const int32_t *build_pay,
+                                        uint64_t build_len,
+                                        const int32_t *probe_key,
+                                        const int32_t *probe_pay,
+                                        uint64_t probe_len,
+                                        fi_join_result *result,
+                                        fi_stream_t stream);
 int fi_radix_join_engine_run_host_int64(fi_radix_join_engine *e,
                                         const int64_t *build_key,
                                         const int64_t *build_pay,
@@ -538,6 +547,53 @@ int fi_datagen_zipf_foreign_keys_int64(int64_t *keys, uint64_t n,
 /* Uniform 64-bit keys. */
 int fi_datagen_uniform_u64_keys(int64_t *keys, uint64_t n, uint64_t seed,
                                 fi_stream_t stream);
+/* Join selectivity (datagen/src/relation.rs:85-151, the `selectivity`
+ * argument of the reference's primary-key generators): every key k of the
+ * column stays when a seeded uniform draw from 0..100, a function of
+ * (seed, k - base), is at most `selectivity` percent, and becomes the null
+ * key (all ones) otherwise.  Applied to primary keys base..base+n-1, a
+ * foreign key f then matches iff f's draw kept it.  selectivity >= 100
+ * keeps every key. */
+int fi_datagen_null_keys_int32(int32_t *keys, uint64_t n, uint32_t selectivity,
+                               uint64_t seed, int32_t base, fi_stream_t stream);
+int fi_datagen_null_keys_int64(int64_t *keys, uint64_t n, uint32_t selectivity,
+                               uint64_t seed, int64_t base, fi_stream_t stream);
+
+/* ---- data sets and relation files (datagen/src/popular.rs,
+ *      radix-join/src/main.rs:657-760, data-store/src/join_data.rs) ----- */
+
+/* The reference's named data sets: primary-key relation R (build) and
+ * uniform foreign-key relation S (probe).  Blanas (SIGMOD 2011):
+ * 16 x 2^20 and 256 x 2^20 tuples, 8-byte keys in the paper; Blanas4MB:
+ * 512 x 2^10 and 256 x 2^20; Kim (PVLDB 2009): 128e6 and 128e6 tuples,
+ * 4-byte keys in the paper; Test: 1000 and 1000; Lutz2Gv32G and
+ * Lutz32Gv32G: 2 GiB and 32 GiB, 32 GiB and 32 GiB of tuples of
+ * tuple_bytes each. */
+typedef enum {
+  FI_DATASET_BLANAS = 0,
+  FI_DATASET_BLANAS4MB = 1,
+  FI_DATASET_KIM = 2,
+  FI_DATASET_TEST = 3,
+  FI_DATASET_LUTZ2GV32G = 4,
+  FI_DATASET_LUTZ32GV32G = 5
+} fi_dataset;
+int fi_dataset_shape(fi_dataset d, uint32_t tuple_bytes, uint64_t *build_len,
+                     uint64_t *probe_len);
+
+/* Relation files of the reference's file-backed join data
+ * (data-store/src/join_data.rs:173-260, build_with_files): one header line,
+ * then one tuple per line, key and payload as decimal integers separated by
+ * one space; a file whose name ends in "gz" is gzip-compressed.  Like the
+ * reference, loading takes two passes: fi_relation_file_len counts the
+ * tuples, fi_relation_file_read_* parses them into caller-owned host columns
+ * of exactly that length.  A malformed line (other than two fields, not a
+ * decimal integer, out of the key type's range) is an InvalidArgument error
+ * naming the file and line; empty lines are skipped.  Host only. */
+int fi_relation_file_len(const char *path, uint64_t *len);
+int fi_relation_file_read_int32(const char *path, int32_t *keys, int32_t *pays,
+                                uint64_t len);
+int fi_relation_file_read_int64(const char *path, int64_t *keys, int64_t *pays,
+                                uint64_t len);
 
 /* ---- autotuner and join server (no reference counterpart; the nearest
  *      reference pieces are the radix-bits heuristic of

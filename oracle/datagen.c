@@ -162,3 +162,25 @@ void dg_uniform_u64_keys(int64_t *keys, uint64_t n, uint64_t seed) {
   for (uint64_t i = 0; i < n; ++i)
     keys[i] = (int64_t)dg_mix64(seed ^ dg_mix64(i + 0x1234567ull));
 }
+
+/* Join selectivity (datagen/src/relation.rs:85-151): a key k stays when a
+ * draw from 0..100, a function of (seed, k - base), is at most selectivity;
+ * otherwise it becomes the null key (all ones).  Null keys stay null. */
+static inline int dg_keep_key(uint64_t seed, uint64_t off, uint32_t selectivity) {
+  return dg_mix64(seed ^ dg_mix64(off + 0x6E756C6Cull)) % 101u <= selectivity;
+}
+void dg_null_keys_i64(int64_t *keys, uint64_t n, uint32_t selectivity,
+                      uint64_t seed, int64_t base) {
+  if (selectivity >= 100) return;
+  for (uint64_t i = 0; i < n; ++i)
+    if (keys[i] != -1 && !dg_keep_key(seed, (uint64_t)(keys[i] - base), selectivity))
+      keys[i] = -1;
+}
+void dg_null_keys_i32(int32_t *keys, uint64_t n, uint32_t selectivity,
+                      uint64_t seed, int32_t base) {
+  if (selectivity >= 100) return;
+  for (uint64_t i = 0; i < n; ++i)
+    if (keys[i] != -1 &&
+        !dg_keep_key(seed, (uint64_t)((int64_t)keys[i] - (int64_t)base), selectivity))
+      keys[i] = -1;
+}

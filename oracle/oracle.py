@@ -209,6 +209,17 @@ def zipf_foreign_keys(n, pk_n, s, seed, pk_seed, dtype=np.int64, base=1):
     return out
 
 
+def null_keys(keys, selectivity, seed, base=1):
+    """In place: keys whose seeded draw exceeds `selectivity` percent become
+    the null key (datagen.c dg_null_keys, the selectivity of
+    datagen/src/relation.rs:85-151)."""
+    ct = C.c_int32 if keys.dtype == np.int32 else C.c_int64
+    getattr(lib(), "dg_null_keys_" + _sfx(keys.dtype))(
+        _p(keys), C.c_uint64(len(keys)), C.c_uint32(selectivity), C.c_uint64(seed),
+        ct(base))
+    return keys
+
+
 def uniform_u64_keys(n, seed):
     out = np.empty(n, np.int64)
     lib().dg_uniform_u64_keys(_p(out), C.c_uint64(n), C.c_uint64(seed))
