@@ -104,14 +104,20 @@ __device__ __forceinline__ void plan_store(uint64_t *p, uint64_t v) {
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// item_start[p] = sum_{q<p} items(q); item_start[F] = total.
+// item_start[p] = sum_{q<p} items(q); item_start[F] = total.  With
+// heavy_cap > 0 (bucket chaining), a partition whose build side exceeds
+// heavy_cap tuples gets no items; it is appended instead to the heavy list
+// that grows down from item_part[item_cap - 1] (*heavy_count entries).  The
+// two fit together: every partition takes at most ceil(probe / width) >= 1
+// entries, and item_cap bounds their sum.
 __global__ void __launch_bounds__(kPlanThreads)
     join_plan_kernel(const uint64_t *__restrict__ build_off, uint64_t build_len,
                      uint32_t build_pad, const uint64_t *__restrict__ probe_off,
                      uint64_t probe_len, uint32_t probe_pad, uint32_t F,
-                     uint32_t width, uint32_t *__restrict__ item_start,
-                     uint32_t *__restrict__ item_part, uint64_t *tile_state,
-                     uint32_t *tile_counter, int *status) {
+                     uint32_t width, uint32_t heavy_cap, uint32_t item_cap,
+                     uint32_t *__restrict__ item_start,
+                     uint32_t *__restrict__ item_part, uint32_t *heavy_count,
+                     uint64_t *tile_state, uint32_t *tile_counter, int *status) {
   __shared__ uint32_t tile_s, prefix_s;
   __shared__ uint32_t warp_tmp[33];
   __shared__ uint32_t vals[kPlanThreads];
@@ -124,7 +130,12 @@ __global__ void __launch_bounds__(kPlanThreads)
     uint64_t bb, be, pb, pe;
     part_bounds(build_off, build_len, build_pad, F, p, bb, be);
     part_bounds(probe_off, probe_len, probe_pad, F, p, pb, pe);
-    if (be > bb && pe > pb) items = (uint32_t)((pe - pb + width - 1) / width);
+    if (be > bb && pe > pb) {
+      if (heavy_cap != 0 && be - bb > heavy_cap)
+        item_part[item_cap - 1u - atomicAdd(heavy_count, 1u)] = p;
+      else
+        items = (uint32_t)((pe - pb + width - 1) / width);
+    }
   }
   vals[threadIdx.x] = items;
   __syncthreads();
@@ -211,7 +222,9 @@ __host__ __device__ inline uint32_t chain_capacity(uint32_t table_bytes,
 // Persistent join: CTA b takes items b, b + grid, b + 2*grid, ...  Items
 // are near-equal in probe work (at most `width` probe tuples each), so the
 // grid stride balances skewed inputs while avoiding a global work counter;
-// the partition of the next item is prefetched.
+// the partition of the next item is prefetched.  With bucket chaining the
+// planner gives no items to partitions whose build side exceeds the table;
+// radix_join_heavy_kernel joins those.
 template <typename K, int kScheme, int kMaxThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
     const Tuple<K> *__restrict__ build, const uint64_t *__restrict__ build_off,
@@ -357,6 +370,96 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
   }
 }
 
+// Heavy partitions (bucket chaining): a partition whose build side exceeds
+// the table was left out of the items and listed at the end of item_part;
+// each becomes R x Q units (build round r of `cap` tuples x probe slice q of
+// at most `width` tuples), numbered consecutively over the list and dealt
+// round-robin to the CTAs.  A partition of tens of millions of equal build
+// keys (e.g. the null keys of a selective data set) is so spread over the
+// whole GPU instead of being joined round after round by one CTA.  Same
+// table layout, launch shape and result slots as radix_join_kernel; with
+// no heavy partition every CTA returns at once.
+template <typename K, int kMaxThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_heavy_kernel(
+    const Tuple<K> *__restrict__ build, const uint64_t *__restrict__ build_off,
+    uint64_t build_len, uint32_t build_pad, const Tuple<K> *__restrict__ probe,
+    const uint64_t *__restrict__ probe_off, uint64_t probe_len,
+    uint32_t probe_pad, uint32_t F, uint32_t ignore_bits,
+    const uint32_t *__restrict__ item_part, uint32_t item_cap,
+    const uint32_t *__restrict__ heavy_count, uint32_t width,
+    uint32_t table_bytes, uint32_t log2_buckets,
+    int64_t *__restrict__ result_set, uint64_t *match_count) {
+  const uint32_t H = *heavy_count;
+  if (H == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t red_tmp[32];
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t cap = chain_capacity<K>(table_bytes, log2_buckets);
+  K *tkeys = reinterpret_cast<K *>(smem_raw);
+  uint16_t *tnext = reinterpret_cast<uint16_t *>(tkeys + cap);
+  uint32_t *heads =
+      reinterpret_cast<uint32_t *>(smem_raw + ((cap * (sizeof(K) + 2) + 15) & ~15u));
+  const uint32_t nbuckets = 1u << log2_buckets;
+  int64_t sum = 0;
+  uint64_t cnt = 0;
+  int64_t cached_p = -1, cached_r = -1;
+  uint64_t g0 = 0;
+  for (uint32_t h = 0; h < H; ++h) {
+    const uint32_t hp = item_part[item_cap - 1u - h];
+    uint64_t bb, be, pb, pe;
+    part_bounds(build_off, build_len, build_pad, F, hp, bb, be);
+    part_bounds(probe_off, probe_len, probe_pad, F, hp, pb, pe);
+    const uint64_t bsize = be - bb, psize = pe - pb;
+    const uint64_t R = (bsize + cap - 1) / cap;
+    const uint64_t Q = (psize + width - 1) / width;
+    const uint64_t per = (psize + Q - 1) / Q;
+    const uint64_t U = R * Q;
+    uint64_t g = g0 + (blockIdx.x + gridDim.x - g0 % gridDim.x) % gridDim.x;
+    for (; g < g0 + U; g += gridDim.x) {
+      const uint64_t u = g - g0, r = u / Q, qi = u % Q;
+      if (!(cached_p == (int64_t)hp && cached_r == (int64_t)r)) {
+        const uint64_t r0 = r * cap;
+        const uint32_t rn = (uint32_t)min((uint64_t)cap, bsize - r0);
+        __syncthreads();  // the previous unit's probe is done with the table
+        for (uint32_t i = tid; i < nbuckets; i += nt) heads[i] = kHeadEnd;
+        __syncthreads();
+        for (uint32_t i = tid; i < rn; i += nt) {
+          const K key = build[bb + r0 + i].key;
+          tkeys[i] = key;
+          const uint32_t old =
+              atomicExch(&heads[chain_bucket(key, ignore_bits, log2_buckets)], i);
+          tnext[i] = (uint16_t)(old == kHeadEnd ? kLinkEnd : old);
+        }
+        __syncthreads();
+        cached_p = hp;
+        cached_r = (int64_t)r;
+      }
+      const uint64_t qb = min(pe, pb + per * qi), qe = min(pe, qb + per);
+      for (uint64_t j = qb + tid; j < qe; j += nt) {
+        const Tuple<K> t = load_tuple_cs(probe + j);
+        uint32_t e = heads[chain_bucket(t.key, ignore_bits, log2_buckets)];
+        if (e == kHeadEnd) continue;
+        for (;;) {
+          if (tkeys[e] == t.key) {
+            sum += static_cast<int64_t>(t.value);
+            cnt += 1;
+          }
+          const uint32_t nx = tnext[e];
+          if (nx == kLinkEnd) break;
+          e = nx;
+        }
+      }
+    }
+    g0 += U;
+  }
+  result_set[(uint64_t)blockIdx.x * nt + tid] += sum;
+  if (match_count != nullptr) {
+    const uint64_t bc = block_reduce_u64(cnt, red_tmp);
+    if (tid == 0 && bc != 0)
+      atomicAdd((unsigned long long *)match_count, (unsigned long long)bc);
+  }
+}
+
 // ---- launchers ---------------------------------------------------------------
 constexpr uint64_t kMinItemWidth = 8192;
 
@@ -396,33 +499,13 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
                               JoinScratch s, uint32_t sm_count,
                               cudaStream_t stream) {
   (void)sm_count;
-  // probe width per item: about four items per CTA for the bulk, never below
-  // kMinItemWidth tuples so that table builds stay amortised
-  const uint64_t probe_tuples =
-      probe_len > (uint64_t)probe_pad * fanout ? probe_len - (uint64_t)probe_pad * fanout : 0;
-  uint64_t width = probe_tuples / ((uint64_t)grid * 4u + 1u);
-  if (width < kMinItemWidth) width = kMinItemWidth;
-  if (width > (1u << 30)) width = 1u << 30;
-  const uint32_t tiles = (fanout + kPlanThreads - 1) / kPlanThreads;
-  cudaError_t e = cudaMemsetAsync(s.tile_state, 0,
-                                  (size_t)(tiles + 1) * sizeof(uint64_t), stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(s.tile_counter, 0, sizeof(uint32_t), stream);
-  if (e != cudaSuccess) return e;
-  join_plan_kernel<<<tiles, kPlanThreads, 0, stream>>>(
-      build_off, build_len, build_pad, probe_off, probe_len, probe_pad, fanout,
-      (uint32_t)width, s.item_start, s.item_part, s.tile_state, s.tile_counter,
-      s.status);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-
   // Several CTAs per SM (an equal share of the shared memory each) when the
   // block allows it, so that one CTA's table build overlaps another's probe:
   // 4 CTAs of <= 256 threads, 2 of <= 512, else one of 1024.
   const uint32_t ctas = join_ctas_per_sm(block);
   const void *fn = scheme == 2 ? join_kernel_ptr<K, 2>(ctas) : join_kernel_ptr<K, 0>(ctas);
   cudaFuncAttributes attr;
-  e = cudaFuncGetAttributes(&attr, fn);
+  cudaError_t e = cudaFuncGetAttributes(&attr, fn);
   if (e != cudaSuccess) return e;
   int dev = 0, per_sm = 0, reserved = 0;
   cudaGetDevice(&dev);
@@ -449,6 +532,29 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   uint32_t lb = 8;
   while (lb < 14 && (1ull << lb) < avg) ++lb;
   while (lb > 8 && chain_capacity<K>(dyn, lb) < avg + avg / 8) --lb;
+  const uint32_t cap = chain_capacity<K>(dyn, lb);
+  if (scheme == 2 && cap == 0) return cudaErrorInvalidValue;
+
+  // probe width per item: about four items per CTA for the bulk, never below
+  // kMinItemWidth tuples so that table builds stay amortised
+  const uint64_t probe_tuples =
+      probe_len > (uint64_t)probe_pad * fanout ? probe_len - (uint64_t)probe_pad * fanout : 0;
+  uint64_t width = probe_tuples / ((uint64_t)grid * 4u + 1u);
+  if (width < kMinItemWidth) width = kMinItemWidth;
+  if (width > (1u << 30)) width = 1u << 30;
+  const uint32_t item_cap = join_items_capacity(fanout, probe_len);
+  uint32_t *heavy_count = s.tile_counter + 1;
+  const uint32_t tiles = (fanout + kPlanThreads - 1) / kPlanThreads;
+  e = cudaMemsetAsync(s.tile_state, 0, (size_t)(tiles + 1) * sizeof(uint64_t), stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.tile_counter, 0, 2 * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  join_plan_kernel<<<tiles, kPlanThreads, 0, stream>>>(
+      build_off, build_len, build_pad, probe_off, probe_len, probe_pad, fanout,
+      (uint32_t)width, scheme == 2 ? cap : 0u, item_cap, s.item_start,
+      s.item_part, heavy_count, s.tile_state, s.tile_counter, s.status);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
 
   const auto *b = reinterpret_cast<const Tuple<K> *>(build);
   const auto *pr = reinterpret_cast<const Tuple<K> *>(probe);
@@ -457,15 +563,32 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
       b, build_off, build_len, build_pad, pr, probe_off, probe_len, probe_pad, \
       fanout, ignore_bits, s.item_start, s.item_part, dyn, lb, result_set,     \
       match_count, s.status)
+#define FI_HEAVY_LAUNCH(T, M)                                                   \
+  do {                                                                          \
+    e = cudaFuncSetAttribute((const void *)radix_join_heavy_kernel<K, T, M>,    \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                             (int)dyn);                                         \
+    if (e != cudaSuccess) return e;                                             \
+    radix_join_heavy_kernel<K, T, M><<<grid, block, dyn, stream>>>(             \
+        b, build_off, build_len, build_pad, pr, probe_off, probe_len,           \
+        probe_pad, fanout, ignore_bits, s.item_part, item_cap, heavy_count,     \
+        (uint32_t)width, dyn, lb, result_set, match_count);                     \
+  } while (0)
   if (scheme == 2) {
     if (ctas == 4) FI_JOIN_LAUNCH(2, 256, 4);
     else if (ctas == 2) FI_JOIN_LAUNCH(2, 512, 2);
     else FI_JOIN_LAUNCH(2, 1024, 1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (ctas == 4) FI_HEAVY_LAUNCH(256, 4);
+    else if (ctas == 2) FI_HEAVY_LAUNCH(512, 2);
+    else FI_HEAVY_LAUNCH(1024, 1);
   } else {
     if (ctas == 4) FI_JOIN_LAUNCH(0, 256, 4);
     else if (ctas == 2) FI_JOIN_LAUNCH(0, 512, 2);
     else FI_JOIN_LAUNCH(0, 1024, 1);
   }
+#undef FI_HEAVY_LAUNCH
 #undef FI_JOIN_LAUNCH
   return cudaGetLastError();
 }
