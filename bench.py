@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
-                    choices=["join", "partition", "ooc", "serve", "dataset"],
+                    choices=["join", "partition", "ooc", "serve", "dataset", "nopart"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
                          "join server against back-to-back plain calls; dataset: "
@@ -69,6 +69,12 @@ def parse():
                          "data set's own")
     ap.add_argument("--selectivity", type=int, default=100,
                     help="dataset workload: join selectivity in percent")
+    ap.add_argument("--ht-scheme", default="linearprobing",
+                    choices=["linearprobing", "perfect"],
+                    help="nopart workload: hash table of the no-partitioning join")
+    ap.add_argument("--ht-dim", default="0,256",
+                    help="nopart workload: grid,block of build and probe (grid 0 "
+                         "= 8 CTAs per SM)")
     ap.add_argument("--ooc-log2n", type=int, default=31,
                     help="out-of-core join: |R| = |S| = 2^ooc_log2n int64 tuples")
     ap.add_argument("--ooc-block", type=int, default=0,
@@ -975,6 +981,103 @@ def run_dataset(a):
         dist.destroy_process_group()
 
 
+def run_nopart(a):
+    """No-partitioning hash join (CudaHashJoin build + probe_sum over a
+    device hash table) on a named data set, Blanas by default: the
+    comparison point for small build sides.  A step re-initialises the table
+    (the reference allocates a fresh one per join), builds and probes.  The
+    table holds 2^floor(log2(2|R|)) entries for linear probing (the
+    reference's load factor 2) and |R|+1 for perfect hashing (keys 1..|R|)."""
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    name, paper_tb = DATASETS[a.data_set]
+    tb = a.tuple_bytes or paper_tb
+    dt = torch.int32 if tb == 8 else torch.int64
+    seed = a.seed + 1000 * rank
+    rk, rp, sk, sp = fi.gen_dataset(getattr(fi.Dataset, name), dt,
+                                    selectivity=a.selectivity, seed=seed)
+    nb, npr = rk.numel(), sk.numel()
+    kept = fi.null_keys(sk.clone(), a.selectivity, seed + 7) != -1
+    exp_s = int(sp.to(torch.int64)[kept].sum().item())
+    del kept
+    perfect = a.ht_scheme == "perfect"
+    scheme = fi.HashingScheme.Perfect if perfect else fi.HashingScheme.LinearProbing
+    # the kernels mask with 2^floor(log2(size)) (as the reference's do), so
+    # the table is a power of two at most half full
+    size = nb + 1 if perfect else 1 << (2 * nb - 1).bit_length()
+    g, blk = [int(x) for x in a.ht_dim.split(",")]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    grid = g or sms * (2048 // blk)
+    ht = fi.HashTable(size, dt)
+    hj = fi.CudaHashJoin(scheme, ht, (grid, blk), (grid, blk),
+                         is_selective=a.selectivity < 100)
+    res = torch.zeros(grid * blk, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    init = getattr(fi.lib(), "fi_hash_table_init_" + ("int32" if tb == 8 else "int64"))
+
+    def step(evs=None):
+        if evs: evs[0].record(stream)
+        fi._check(init(fi._ptr(ht.mem), fi.C.c_uint64(ht.mem.shape[0]), fi._stream(None)))
+        hj.build(rk, rp)
+        if evs: evs[1].record(stream)
+        hj.probe_sum(sk, sp, res)
+        if evs: evs[2].record(stream)
+
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        res.zero_()
+        step()
+        verified = verified and int(res.sum().item()) == exp_s
+    K = a.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    res.zero_()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(K):
+            step(ev[k])
+        torch.cuda.synchronize()
+        barrier(world)
+    tot = int(res.sum().item())
+    verified = verified and tot == (exp_s * K + (1 << 63)) % (1 << 64) - (1 << 63)
+    build_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    probe_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    ms = max_over_ranks(build_ms + probe_ms, world)
+    value = world * (nb + npr) / (ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    # algorithmic bytes: table init (one entry per slot), build (read a tuple,
+    # write an entry), probe (read a tuple, read an entry)
+    build_bytes = size * tb + nb * 2 * tb
+    probe_bytes = npr * 2 * tb
+    if rank == 0:
+        line = {"metric": "no-partitioning join G tuples/s", "value": value,
+                "unit": UNIT, "n_gpus": world, "steps": K, "warmup": a.warmup,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32" if tb == 8 else "int64",
+                "data": "synthetic %s data set (seeded permutation PK, uniform FK, "
+                        "payload = key)" % name,
+                "config": {"workload": "nopart_join_%s_%s_%s" % (
+                               a.data_set, "int32" if tb == 8 else "int64", a.ht_scheme),
+                           "build_tuples": nb, "probe_tuples": npr,
+                           "hash_table_entries": size, "grid": grid, "block": blk,
+                           "l2_flush": "none: probe input larger than L2"},
+                "phases": {"init_build": {"ms": build_ms,
+                                          "gb_per_s": build_bytes / (build_ms / 1e3) / 1e9},
+                           "probe": {"ms": probe_ms,
+                                     "gb_per_s": probe_bytes / (probe_ms / 1e3) / 1e9}},
+                "roofline": {"bound": "hbm", "kernel": "probe",
+                             "achieved": probe_bytes / (probe_ms / 1e3) / 1e9,
+                             "peak": peak, "unit": "GB/s",
+                             "frac": probe_bytes / (probe_ms / 1e3) / 1e9 / peak,
+                             "peak_source": peak_kind, "traffic": None},
+                "clocks": clk.summary(), "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -987,6 +1090,8 @@ def main():
         run_serve(a)
     elif a.workload == "dataset":
         run_dataset(a)
+    elif a.workload == "nopart":
+        run_nopart(a)
     else:
         run_ours(a)
 

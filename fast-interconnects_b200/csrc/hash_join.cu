@@ -12,6 +12,16 @@
 // B200 specifics: whole entries are read with one 8/16-byte load, probe keys
 // and payloads with evict-first loads, and keys outside [0, size) are skipped
 // by the perfect scheme instead of addressing out of bounds.
+//
+// Measured on B200 (Blanas: 16M x 256M int64, 1184 x 256 threads): linear
+// probing builds in 1.0 ms and probes in 11.1 ms (a 2^25-entry, 512 MB
+// table: one random access per probe, far beyond the 126 MB L2), perfect
+// hashing probes in 4.7 ms (16M + 1 entries).  Four tuples per thread with
+// their table loads issued together made it no faster (11.7 ms): the probe
+// is bound by random HBM accesses, not by their latency.  The table size
+// matters more: the hash masks with 2^floor(log2(size)) (as the reference
+// does), so a size that is not a power of two can fill the table to near
+// 1 (Kim, 128e6 keys in 2^27 slots: 27 ms per probe against 5.8 ms in 2^28).
 #include "common.cuh"
 #include "kernels.h"
 
