@@ -12,8 +12,8 @@
 //      shared-memory table each; the 1024M x 1024M int64 join runs fastest
 //      with 2^30 / 2^18), one pass up to 11 bits and two balanced passes
 //      above (a single pass loses its write combining above 11 bits on
-//      B200), bucket chaining, 256-thread join CTAs (four per SM), TMA-fed
-//      scatters.
+//      B200), bucket chaining, the join shape chosen by partition size
+//      (join_auto_block), TMA-fed scatters.
 // Joins below small_tuples in total go to batches.
 #include <cmath>
 #include <cstdio>
@@ -64,7 +64,7 @@ void autotune_model(uint64_t build_len, fi_tuned_plan *out) {
   }
   out->radix_bits.pass_bits[2] = -1;
   out->hashing_scheme = FI_HASHING_BUCKET_CHAINING;
-  out->join_block = 256;
+  out->join_block = 0;  // by partition size (join_auto_block)
   out->scatter = 0;
 }
 
@@ -134,7 +134,8 @@ extern "C" int fi_autotune_load(const char *path) {
           (e.tuple_bytes != 8 && e.tuple_bytes != 16) || e.bits1 < 0 ||
           e.bits1 > 14 || e.bits2 > 10 ||
           (e.scheme != FI_HASHING_PERFECT && e.scheme != FI_HASHING_BUCKET_CHAINING) ||
-          (e.join_block != 256 && e.join_block != 512 && e.join_block != 1024) ||
+          (e.join_block != 0 && e.join_block != 256 && e.join_block != 512 &&
+           e.join_block != 1024) ||
           e.scatter > 1) {
         std::fclose(f);
         return set_error(FI_ERR_INVALID_ARGUMENT, "%s:%d: malformed tuning entry",

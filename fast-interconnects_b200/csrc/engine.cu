@@ -12,7 +12,7 @@
 //   2. Tile scatter of R and S into chunked AoS relations (pass 1).
 //   3. Plan: per first-pass partition p1, its length (summed over chunks),
 //      its start in the pass-2 output and its split into "pieces" of at most
-//      kPieceTuples tuples.  Pieces are the unit of pass-2 work, so a
+//      piece_tuples(len) tuples.  Pieces are the unit of pass-2 work, so a
 //      Zipf-hot partition is spread over many CTAs.
 //   4. Piece histograms on the second-pass bits (reads the pass-1 output).
 //   5. Cursors: per (p1, p2) the contiguous output offsets, per piece its
@@ -36,12 +36,21 @@
 
 namespace fi {
 
-// Pass-2 piece length.  Measured on B200 (1024M x 1024M int64, 9+9 bits,
-// per relation): 2^17 -> pass-2 histogram 3.01 ms, scatter 7.31 ms; 2^18 ->
-// 2.93 and 7.02 ms; 2^19 -> 3.08 and 6.91; 2^20 -> 3.05 and 6.85 (longer
-// pieces amortise a scatter CTA's set-up, shorter ones give the histogram
-// more CTAs).
-constexpr uint64_t kPieceTuples = 1ull << 18;
+// Pass-2 piece length: about four pieces per SM, between 2^13 and 2^18
+// tuples.  Measured on B200 (1024M x 1024M int64, 9+9 bits, per relation):
+// 2^17 -> pass-2 histogram 3.01 ms, scatter 7.31 ms; 2^18 -> 2.93 and 7.02
+// ms; 2^19 -> 3.08 and 6.91; 2^20 -> 3.05 and 6.85 (longer pieces amortise a
+// scatter CTA's set-up, shorter ones give the histogram more CTAs).  Small
+// relations need shorter pieces to fill the GPU: 16M int32 tuples at 6+6
+// bits made only 64 pieces of 2^18 (pass-2 histogram 0.36 ms, scatter 0.22).
+constexpr uint64_t kMaxPieceTuples = 1ull << 18;
+constexpr uint64_t kMinPieceTuples = 1ull << 13;
+inline uint64_t piece_tuples(uint64_t len, uint32_t sm_count) {
+  const uint64_t want = len / (4ull * sm_count);
+  uint64_t p = kMinPieceTuples;
+  while (p < kMaxPieceTuples && 2 * p <= want) p *= 2;
+  return p;
+}
 // First-pass chunks per SM and the pass-2 tile shape.  Measured on B200
 // (1024M x 1024M int64, 9+9 bits): the wide shape (512 threads, 4096-tuple
 // tiles, one CTA per SM) beats two 256-thread CTAs per SM with 2048-tuple
@@ -50,18 +59,18 @@ constexpr uint64_t kPieceTuples = 1ull << 18;
 constexpr uint32_t kChunksPerSm = 1;
 template <typename K>
 using Pass2Shape = TileWide<K>;
-// join launch: four CTAs of 256 threads per SM for bucket chaining
-// (measured on B200, 1024M x 1024M int64, 9+9 bits: join 7.48 ms, against
-// 7.78 ms with two CTAs of 512 and 9.75 ms with one of 1024); two CTAs of
-// 512 for the perfect scheme, whose table must span the largest key of a
-// partition: half the SM's shared memory holds ~14.5K int64 keys, the
-// capacity of the reference's one-table-per-CTA sizing
-// (radix-join/src/cuda_radix_join.rs:234-237)
-constexpr uint32_t kJoinBlock = 256;
+// Join launch when the plan leaves it open (join block 0).  Bucket
+// chaining: the most CTAs per SM whose table still holds an average
+// partition (join_auto_block): four of 256 threads for the 4K-tuple
+// partitions of 1024M x 1024M int64 at 9+9 bits (join 7.48 ms, against 7.78
+// ms with two CTAs of 512 and 9.75 ms with one of 1024), one of 1024 for the
+// 16K-tuple int32 partitions of 16M x 16M at 10 bits (0.12 ms, against 2.0
+// ms when the 256-thread tables are too small and every partition is joined
+// in rounds).  Perfect hashing: two CTAs of 512, whose table must span the
+// largest key of a partition: half the SM's shared memory holds ~14.5K
+// int64 keys, the capacity of the reference's one-table-per-CTA sizing
+// (radix-join/src/cuda_radix_join.rs:234-237).
 constexpr uint32_t kJoinBlockPerfect = 512;
-inline uint32_t default_join_block(fi_hashing_scheme s) {
-  return s == FI_HASHING_PERFECT ? kJoinBlockPerfect : kJoinBlock;
-}
 
 struct Pass2Plan {
   uint64_t *reg_pre;      // [F1][C1+1] prefix of the chunk regions of p1
@@ -70,6 +79,7 @@ struct Pass2Plan {
   uint32_t *hist;         // [max_pieces][F2]
   uint64_t *cursor;       // [max_pieces][F2]
   uint64_t *off2;         // [F1*F2 + 1]
+  uint32_t piece_log2;    // tuples per piece = 2^piece_log2 (piece_tuples)
 };
 
 // Exclusive scan of a global u64 array by one CTA; a[n] gets the total.
@@ -104,7 +114,7 @@ __global__ void __launch_bounds__(1024)
     }
     rp[C1] = run;
     pl.p1_base[p1] = run;
-    piece_count_tmp[p1] = (run + kPieceTuples - 1) / kPieceTuples;
+    piece_count_tmp[p1] = (run + (1ull << pl.piece_log2) - 1) >> pl.piece_log2;
   }
   __syncthreads();
   cta_scan_global_u64(pl.p1_base, F1, tmp);
@@ -138,8 +148,8 @@ __global__ void __launch_bounds__(512)
   if (k >= total) return;
   const uint32_t p1 = find_p1(pl.piece_first, F1, k);
   const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
-  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
-  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) << pl.piece_log2;
+  const uint64_t s1 = min(n, s0 + ((uint64_t)1 << pl.piece_log2));
   for (uint32_t i = threadIdx.x; i < F2; i += blockDim.x) hist[i] = 0;
   __syncthreads();
   const uint64_t *rp = pl.reg_pre + (uint64_t)p1 * (C1 + 1);
@@ -210,8 +220,8 @@ __global__ void __launch_bounds__(Pass2Shape<K>::kThreads, Pass2Shape<K>::kMinBl
   if (k >= total) return;
   const uint32_t p1 = find_p1(pl.piece_first, F1, k);
   const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
-  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
-  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) << pl.piece_log2;
+  const uint64_t s1 = min(n, s0 + ((uint64_t)1 << pl.piece_log2));
   const uint64_t *cp = pl.cursor + (uint64_t)k * F2;
   const uint64_t base = cp[0];
   for (uint32_t p = threadIdx.x; p < F2; p += blockDim.x) {
@@ -261,8 +271,8 @@ __global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
   if (k >= total) return;
   const uint32_t p1 = find_p1(pl.piece_first, F1, k);
   const uint64_t n = pl.p1_base[p1 + 1] - pl.p1_base[p1];
-  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) * kPieceTuples;
-  const uint64_t s1 = min(n, s0 + kPieceTuples);
+  const uint64_t s0 = (uint64_t)(k - pl.piece_first[p1]) << pl.piece_log2;
+  const uint64_t s1 = min(n, s0 + ((uint64_t)1 << pl.piece_log2));
   const uint64_t *cp = pl.cursor + (uint64_t)k * F2;
   const uint64_t base = cp[0];
   for (uint32_t p = threadIdx.x; p < F2; p += blockDim.x)
@@ -317,7 +327,7 @@ struct fi_radix_join_engine {
   int32_t bits1, bits2;   // current plan; bits2 < 0: single pass
   int32_t cap1, cap2;     // bits the buffers were sized for
   fi_hashing_scheme scheme;
-  uint32_t join_block = kJoinBlock;
+  uint32_t join_block = 0;  // as planned; 0 = by scheme and partition size
   uint32_t scatter = 0;   // 0: TMA-fed where possible, 1: register-fed
   uint32_t sm_count, C1, F1, F2, max_pieces;
   DevBuf rel1[2], off1[2], loc1[2], rel2[2];
@@ -328,7 +338,13 @@ struct fi_radix_join_engine {
   int scatter_variant() const {
     return scatter == 1 ? kScatterRegisters : kScatterAuto;
   }
-  uint32_t join_grid() const { return sm_count * join_ctas_per_sm(join_block); }
+  // join shape of a run over `build` tuples in `fanout` partitions
+  template <typename K>
+  uint32_t join_block_for(uint64_t build, uint32_t fanout) const {
+    if (join_block) return join_block;
+    return scheme == FI_HASHING_PERFECT ? kJoinBlockPerfect
+                                        : join_auto_block<K>(build, fanout);
+  }
   DevBuf in_cols[4];  // device copies of host input (run_host)
   uint64_t part_len[2] = {0, 0};  // lengths of the partitioned relations
   bool built = false;             // a build relation is partitioned
@@ -355,10 +371,12 @@ struct fi_radix_join_engine {
     return HistScratch{(uint32_t *)hist_scratch.ptr, (uint64_t *)tile_state.ptr,
                        (uint32_t *)counters.ptr, (int *)status.ptr};
   }
-  Pass2Plan plan(int r) {
+  Pass2Plan plan(int r, uint64_t piece) {
+    uint32_t lg = 0;
+    while ((1ull << lg) < piece) ++lg;
     return Pass2Plan{(uint64_t *)reg_pre[r].ptr, (uint64_t *)p1_base[r].ptr,
                      (uint32_t *)piece_first[r].ptr, (uint32_t *)hist2[r].ptr,
-                     (uint64_t *)cursor2[r].ptr, (uint64_t *)off2[r].ptr};
+                     (uint64_t *)cursor2[r].ptr, (uint64_t *)off2[r].ptr, lg};
   }
   void release_all() {
     for (int r = 0; r < 2; ++r) {
@@ -415,13 +433,17 @@ extern "C" int fi_radix_join_engine_new(uint64_t max_build_len,
   e->bits1 = e->cap1 = b1;
   e->bits2 = e->cap2 = b2;
   e->scheme = hashing_scheme;
-  e->join_block = default_join_block(hashing_scheme);
   e->sm_count = (uint32_t)device_sm_count();
   e->C1 = e->sm_count * kChunksPerSm;
   e->F1 = 1u << b1;
   e->F2 = b2 >= 0 ? (1u << b2) : 1u;
   const uint64_t maxn = std::max(max_build_len, max_probe_len);
-  e->max_pieces = (uint32_t)((maxn + kPieceTuples - 1) / kPieceTuples + e->F1);
+  // pieces of a relation of len <= maxn tuples: at most len / piece + F1,
+  // and len / piece_tuples(len) stays below 8 per SM or maxn / 2^18
+  e->max_pieces = (uint32_t)(std::max<uint64_t>(8ull * e->sm_count,
+                                                 (maxn + kMaxPieceTuples - 1) /
+                                                     kMaxPieceTuples) +
+                             e->F1 + 1);
   const uint64_t pad = kPaddingBytes / tuple_bytes;
   const uint32_t pass1_chunks = b2 >= 0 ? e->C1 : 1;
   int rc = FI_OK;
@@ -512,7 +534,7 @@ static int engine_pass2(fi_radix_join_engine *e, int r, uint32_t C1,
   const uint32_t b1 = (uint32_t)e->bits1;
   const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
   const uint64_t mask2 = (uint64_t)(F2 - 1u) << b1;
-  Pass2Plan pl = e->plan(r);
+  Pass2Plan pl = e->plan(r, piece_tuples(len, e->sm_count));
   pass2_plan_kernel<<<1, 1024, 0, st>>>((const uint64_t *)e->off1[r].ptr, C1, F1,
                                         padded1, pad, pl,
                                         (uint64_t *)e->piece_tmp[r].ptr);
@@ -618,6 +640,9 @@ static int engine_join(fi_radix_join_engine *e, fi_join_result *result,
   JoinScratch js{(uint32_t *)e->join_items.ptr, (uint32_t *)e->join_part.ptr,
                  (uint64_t *)e->join_tiles.ptr, (uint32_t *)e->join_counters.ptr,
                  (int *)e->status.ptr};
+  const uint32_t jb =
+      e->join_block_for<K>(e->part_len[0], e->bits2 < 0 ? e->F1 : e->F1 * e->F2);
+  const uint32_t grid = e->sm_count * join_ctas_per_sm(jb);
   if (e->bits2 < 0) {
     const uint32_t pad = kPaddingBytes / sizeof(Tuple<K>);
     const uint64_t padded[2] = {e->part_len[0] + (uint64_t)e->F1 * pad,
@@ -625,8 +650,8 @@ static int engine_join(fi_radix_join_engine *e, fi_join_result *result,
     FI_CK(launch_radix_join<K>(e->rel1[0].ptr, (const uint64_t *)e->off1[0].ptr,
                                padded[0], pad, e->rel1[1].ptr,
                                (const uint64_t *)e->off1[1].ptr, padded[1], pad,
-                               e->F1, (uint32_t)e->bits1, scheme, e->join_grid(),
-                               e->join_block, (int64_t *)e->join_sums.ptr,
+                               e->F1, (uint32_t)e->bits1, scheme, grid, jb,
+                               (int64_t *)e->join_sums.ptr,
                                (uint64_t *)e->join_count.ptr, js, e->sm_count,
                                st),
           "join");
@@ -635,15 +660,14 @@ static int engine_join(fi_radix_join_engine *e, fi_join_result *result,
                                e->part_len[0], 0, e->rel2[1].ptr,
                                (const uint64_t *)e->off2[1].ptr, e->part_len[1], 0,
                                e->F1 * e->F2, (uint32_t)(e->bits1 + e->bits2),
-                               scheme, e->join_grid(), e->join_block,
-                               (int64_t *)e->join_sums.ptr,
+                               scheme, grid, jb, (int64_t *)e->join_sums.ptr,
                                (uint64_t *)e->join_count.ptr, js, e->sm_count,
                                st),
           "join");
   }
   e->mark(9, st);
   finish_result_kernel<<<1, 1024, 0, st>>>(
-      (const int64_t *)e->join_sums.ptr, (uint64_t)e->join_grid() * e->join_block,
+      (const int64_t *)e->join_sums.ptr, (uint64_t)grid * jb,
       (const uint64_t *)e->join_count.ptr, result);
   FI_CK(cudaGetLastError(), "result");
   e->launches += 3;  // join plan, join, result
@@ -845,10 +869,10 @@ extern "C" int fi_radix_join_engine_set_plan(fi_radix_join_engine *e,
       plan->hashing_scheme != FI_HASHING_BUCKET_CHAINING)
     return set_error(FI_ERR_UNSUPPORTED,
                      "the radix join supports Perfect and BucketChaining");
-  const uint32_t jb =
-      plan->join_block ? plan->join_block : default_join_block(plan->hashing_scheme);
-  if (jb != 256 && jb != 512 && jb != 1024)
-    return set_error(FI_ERR_INVALID_ARGUMENT, "join_block must be 256, 512 or 1024");
+  const uint32_t jb = plan->join_block;
+  if (jb != 0 && jb != 256 && jb != 512 && jb != 1024)
+    return set_error(FI_ERR_INVALID_ARGUMENT,
+                     "join_block must be 0 (by partition size), 256, 512 or 1024");
   if (plan->scatter > 1)
     return set_error(FI_ERR_INVALID_ARGUMENT, "unknown scatter variant");
   e->bits1 = b1;

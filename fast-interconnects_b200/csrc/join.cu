@@ -488,6 +488,54 @@ uint32_t join_ctas_per_sm(uint32_t block) {
   return block <= 256 ? 4u : block <= 512 ? 2u : 1u;
 }
 
+// Dynamic shared memory of one join CTA when `ctas` share an SM.
+template <typename K, int kScheme>
+static uint32_t join_dyn_smem(uint32_t ctas) {
+  cudaFuncAttributes attr;
+  if (cudaFuncGetAttributes(&attr, join_kernel_ptr<K, kScheme>(ctas)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int dev = 0, per_sm = 0, reserved = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  uint32_t dyn = (uint32_t)device_max_smem_optin() - (uint32_t)attr.sharedSizeBytes;
+  if (ctas > 1) {
+    const int share = per_sm / (int)ctas - reserved - (int)attr.sharedSizeBytes;
+    if (share > 0 && (uint32_t)share < dyn) dyn = (uint32_t)share;
+  }
+  return dyn & ~127u;
+}
+
+// Bucket count of the chaining table for an average build partition `avg`:
+// the next power of two above it, then fewer only while the table would not
+// hold it with 1/8 headroom.
+template <typename K>
+static uint32_t join_log2_buckets(uint32_t dyn, uint64_t avg) {
+  uint32_t lb = 8;
+  while (lb < 14 && (1ull << lb) < avg) ++lb;
+  while (lb > 8 && chain_capacity<K>(dyn, lb) < avg + avg / 8) --lb;
+  return lb;
+}
+
+// A shape fits when its table holds an average partition with 1/8 headroom
+// and at most about two keys per bucket (2^(floor(log2 avg) - 1) buckets or
+// more): fewer buckets make chains that cost more than the extra CTAs win.
+template <typename K>
+uint32_t join_auto_block(uint64_t build_tuples, uint32_t fanout) {
+  const uint64_t avg = build_tuples / (fanout ? fanout : 1) + 1;
+  uint32_t lb_min = 0;
+  while ((2ull << lb_min) <= avg) ++lb_min;  // floor(log2 avg)
+  lb_min = lb_min > 9 ? lb_min - 1 : 8;
+  if (lb_min > 14) lb_min = 14;
+  for (uint32_t block : {256u, 512u}) {
+    const uint32_t dyn = join_dyn_smem<K, 2>(join_ctas_per_sm(block));
+    if (dyn && chain_capacity<K>(dyn, lb_min) >= avg + avg / 8) return block;
+  }
+  return 1024;
+}
+
 template <typename K>
 cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
                               uint64_t build_len, uint32_t build_pad,
@@ -504,34 +552,22 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   // 4 CTAs of <= 256 threads, 2 of <= 512, else one of 1024.
   const uint32_t ctas = join_ctas_per_sm(block);
   const void *fn = scheme == 2 ? join_kernel_ptr<K, 2>(ctas) : join_kernel_ptr<K, 0>(ctas);
-  cudaFuncAttributes attr;
-  cudaError_t e = cudaFuncGetAttributes(&attr, fn);
-  if (e != cudaSuccess) return e;
-  int dev = 0, per_sm = 0, reserved = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-  uint32_t dyn = (uint32_t)device_max_smem_optin() - (uint32_t)attr.sharedSizeBytes;
-  if (ctas > 1) {
-    const int share = per_sm / (int)ctas - reserved - (int)attr.sharedSizeBytes;
-    if (share > 0 && (uint32_t)share < dyn) dyn = (uint32_t)share;
-  }
-  dyn &= ~127u;
-  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  const uint32_t dyn =
+      scheme == 2 ? join_dyn_smem<K, 2>(ctas) : join_dyn_smem<K, 0>(ctas);
+  if (dyn == 0) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
 
-  // buckets: the next power of two above the average build partition, then
-  // fewer only while the table would not hold an average partition with
-  // 1/8 headroom.  A larger build side is joined in rounds; asking for twice
-  // the average instead cut 8K-tuple partitions down to 256 buckets, and the
-  // 32-entry chains made the join of 2^28 x 2^30 int64 tuples 7x slower
-  // (36.7 ms against 4.4-5.5 ms with short chains, measured on B200).
+  // buckets (join_log2_buckets): a larger build side is joined in rounds;
+  // asking for twice the average instead cut 8K-tuple partitions down to
+  // 256 buckets, and the 32-entry chains made the join of 2^28 x 2^30 int64
+  // tuples 7x slower (36.7 ms against 4.4-5.5 ms with short chains,
+  // measured on B200).
   const uint64_t build_tuples =
       build_len > (uint64_t)build_pad * fanout ? build_len - (uint64_t)build_pad * fanout : 0;
   const uint64_t avg = build_tuples / fanout + 1;
-  uint32_t lb = 8;
-  while (lb < 14 && (1ull << lb) < avg) ++lb;
-  while (lb > 8 && chain_capacity<K>(dyn, lb) < avg + avg / 8) --lb;
+  const uint32_t lb = join_log2_buckets<K>(dyn, avg);
   const uint32_t cap = chain_capacity<K>(dyn, lb);
   if (scheme == 2 && cap == 0) return cudaErrorInvalidValue;
 
@@ -604,5 +640,7 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
 
 FI_INSTANTIATE_JOIN(int32_t)
 FI_INSTANTIATE_JOIN(int64_t)
+template uint32_t join_auto_block<int32_t>(uint64_t, uint32_t);
+template uint32_t join_auto_block<int64_t>(uint64_t, uint32_t);
 
 }  // namespace fi

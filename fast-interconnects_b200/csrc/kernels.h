@@ -121,6 +121,11 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
 uint32_t join_items_capacity(uint32_t fanout, uint64_t probe_len);
 // CTAs of `block` threads the join runs per SM (4, 2 or 1).
 uint32_t join_ctas_per_sm(uint32_t block);
+// Bucket-chaining join shape for `build_tuples` over `fanout` partitions:
+// the block (256, 512 or 1024 threads) with the most CTAs per SM whose
+// shared-memory table still holds an average partition with 1/8 headroom.
+template <typename K>
+uint32_t join_auto_block(uint64_t build_tuples, uint32_t fanout);
 
 // ---- no-partitioning join ------------------------------------------------
 template <typename K>

@@ -368,8 +368,9 @@ uint64_t fi_radix_join_engine_workspace_bytes(const fi_radix_join_engine *e);
  * engine's buffers were sized for the radix bits given at creation; a plan
  * may use fewer bits per pass, one pass instead of two, and tuples no
  * larger than the creation's tuple_bytes.  join_block: threads per join CTA
- * (256: four CTAs per SM, 512: two, 1024: one; 0 = 256 for BucketChaining,
- * 512 for Perfect, whose table then holds ~14.5K int64 keys).  scatter: 0 = tile scatter fed by TMA bulk
+ * (256: four CTAs per SM, 512: two, 1024: one), or 0: for BucketChaining the
+ * most CTAs per SM whose shared-memory table holds an average partition with
+ * 1/8 headroom, for Perfect 512 (a table of ~14.5K int64 keys).  scatter: 0 = tile scatter fed by TMA bulk
  * copies where the columns allow it, 1 = fed by register loads.  Setting a
  * plan drops a resident build side. */
 typedef struct {
