@@ -61,9 +61,12 @@ def parse():
                          "join server against back-to-back plain calls; dataset: "
                          "a named data set of the reference (--data-set)")
     ap.add_argument("--data-set", default="blanas",
-                    choices=["blanas", "blanas4mb", "kim", "lutz2gv32g", "lutz32gv32g"],
+                    choices=["blanas", "blanas4mb", "kim", "lutz2gv32g", "lutz32gv32g",
+                             "custom"],
                     help="dataset workload: Blanas 16M x 256M int64, Kim 128e6 x "
-                         "128e6 int32 (the papers' key sizes), ...")
+                         "128e6 int32 (the papers' key sizes), ...; custom: |R| = |S| "
+                         "= 2^log2n with --zipf and --bits (e.g. the 16M x 16M int32 "
+                         "one-pass join: --log2n 24 --bits 10 --tuple-bytes 8)")
     ap.add_argument("--tuple-bytes", type=int, default=0,
                     help="dataset workload: 8 (int32) or 16 (int64); 0 = the "
                          "data set's own")
@@ -876,7 +879,21 @@ def run_serve(a):
 
 DATASETS = {  # name -> (fi.Dataset member, tuple bytes of the paper)
     "blanas": ("Blanas", 16), "blanas4mb": ("Blanas4MB", 16), "kim": ("Kim", 8),
-    "lutz2gv32g": ("Lutz2Gv32G", 16), "lutz32gv32g": ("Lutz32Gv32G", 16)}
+    "lutz2gv32g": ("Lutz2Gv32G", 16), "lutz32gv32g": ("Lutz32Gv32G", 16),
+    "custom": ("Custom", 16)}
+
+
+def gen_custom(fi, torch, a, dt, seed):
+    """The reference's Custom data set (radix-join/src/main.rs:727-757):
+    |R| = |S| = 2^log2n, primary keys with the join selectivity, foreign keys
+    uniform or Zipf(--zipf) over them; payload = key."""
+    n = 1 << a.log2n
+    rk = torch.empty(n, dtype=dt, device="cuda")
+    sk = torch.empty(n, dtype=dt, device="cuda")
+    fi.gen_primary_keys(rk, seed)
+    fi.null_keys(rk, a.selectivity, seed + 7)
+    fi.gen_zipf_foreign_keys(sk, n, a.zipf, seed + 1, seed)
+    return rk, rk.clone(), sk, sk.clone()
 
 
 def run_dataset(a):
@@ -890,9 +907,12 @@ def run_dataset(a):
     name, paper_tb = DATASETS[a.data_set]
     tb = a.tuple_bytes or paper_tb
     dt = torch.int32 if tb == 8 else torch.int64
-    ds = getattr(fi.Dataset, name)
     seed = a.seed + 1000 * rank
-    rk, rp, sk, sp = fi.gen_dataset(ds, dt, selectivity=a.selectivity, seed=seed)
+    if name == "Custom":
+        rk, rp, sk, sp = gen_custom(fi, torch, a, dt, seed)
+    else:
+        rk, rp, sk, sp = fi.gen_dataset(getattr(fi.Dataset, name), dt,
+                                        selectivity=a.selectivity, seed=seed)
     nb, npr = rk.numel(), sk.numel()
     kept = fi.null_keys(sk.clone(), a.selectivity, seed + 7) != -1
     exp_c = int(kept.sum().item())
@@ -900,6 +920,9 @@ def run_dataset(a):
     del kept
     plan = fi.autotune_plan(tb, nb, npr, small_tuples=1)
     bits = plan["bits"] if plan["bits"] and plan["bits"][0] > 0 else (1,)
+    if name == "Custom":  # the given bits, default join shape and scatter
+        bits = tuple(int(x) for x in a.bits.split(","))
+        plan = dict(plan, join_block=0, scatter=0)
     engine = fi.RadixJoinEngine(nb, npr, dt, fi.RadixBits(*bits),
                                 fi.HashingScheme.BucketChaining)
     engine.set_plan(fi.RadixBits(*bits), fi.HashingScheme.BucketChaining,
@@ -961,7 +984,9 @@ def run_dataset(a):
                 "data": "synthetic %s data set (seeded permutation PK with %d%% "
                         "selectivity, uniform FK, payload = key)" % (name, a.selectivity),
                 "config": {"workload": "radix_join_%s_%s_sel%d" % (
-                               a.data_set, "int32" if tb == 8 else "int64", a.selectivity),
+                               a.data_set if name != "Custom" else "%dMx%dM_%sbits_zipf%.1f" % (
+                                   nb >> 20, npr >> 20, "+".join(str(b) for b in bits), a.zipf),
+                               "int32" if tb == 8 else "int64", a.selectivity),
                            "build_tuples": nb, "probe_tuples": npr,
                            "radix_bits": list(bits), "hashing_scheme": "chaining",
                            "join_block": plan["join_block"],
