@@ -377,6 +377,95 @@ class GpuRadixPartitioner:
 # ---------------------------------------------------------------------------
 # CudaRadixJoin
 # ---------------------------------------------------------------------------
+class CpuHistogramAlgorithm(enum.IntEnum):
+    Chunked = 0
+    ChunkedSimd = 1
+
+
+class CpuRadixPartitionAlgorithm(enum.IntEnum):
+    NC = 0
+    SWWC = 1
+    SWWCSimd = 2
+
+
+class CpuRadixPartitioner:
+    """CpuRadixPartitioner (cpu_radix_partition.rs): per-chunk prefix sum and
+    partition on the host, one partitioner per thread.  Arrays are numpy
+    arrays or CPU tensors; `relation` is a (padded_len, 2) array of the key
+    type."""
+
+    def __init__(self, histogram_algorithm, partition_algorithm, radix_bits):
+        self.radix_bits = radix_bits
+        self.h = C.c_void_p()
+        _check(lib().fi_cpu_radix_partitioner_new(
+            C.c_int(int(histogram_algorithm)), C.c_int(int(partition_algorithm)),
+            C.c_uint32(radix_bits), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_cpu_radix_partitioner_free(self.h)
+            self.h = None
+
+    @staticmethod
+    def _addr(a):
+        return C.c_void_p(a.data_ptr() if isinstance(a, torch.Tensor) else a.ctypes.data)
+
+    @staticmethod
+    def _sfx(a):
+        return "int32" if a.dtype in (torch.int32, np_int32()) else "int64"
+
+    def prefix_sum(self, keys, chunk_id, num_chunks, chunk_offsets, ignore_bits=0):
+        f = getattr(lib(), "fi_cpu_prefix_sum_" + self._sfx(keys))
+        _check(f(self.h, self._addr(keys), C.c_uint64(len(keys)), C.c_uint32(chunk_id),
+                 C.c_uint32(num_chunks), C.c_uint32(ignore_bits),
+                 self._addr(chunk_offsets)))
+
+    def partition(self, keys, pays, chunk_id, num_chunks, chunk_offsets, relation,
+                  ignore_bits=0):
+        f = getattr(lib(), "fi_cpu_partition_" + self._sfx(keys))
+        _check(f(self.h, self._addr(keys), self._addr(pays), C.c_uint64(len(keys)),
+                 C.c_uint32(chunk_id), C.c_uint32(num_chunks), C.c_uint32(ignore_bits),
+                 self._addr(chunk_offsets), self._addr(relation),
+                 C.c_uint64(len(relation))))
+
+
+def np_int32():
+    import numpy as np
+    return np.dtype(np.int32)
+
+
+def cpu_radix_partition(keys, pays, radix_bits, num_chunks,
+                        algorithm=CpuRadixPartitionAlgorithm.SWWC, fill=-1):
+    """Chunked partition of numpy columns on num_chunks host threads (one
+    partitioner each, as the reference's rayon scope): returns (relation of
+    len + chunks*F*pad tuples, offsets of chunks*F entries)."""
+    import threading
+    import numpy as np
+    F = 1 << radix_bits
+    pad = padding_len(torch.int32 if keys.dtype == np.int32 else torch.int64)
+    offsets = np.zeros(num_chunks * F, np.uint64)
+    rel = np.full((len(keys) + num_chunks * F * pad, 2), fill, keys.dtype)
+    errors = []
+
+    def run(c):
+        try:
+            p = CpuRadixPartitioner(CpuHistogramAlgorithm.Chunked, algorithm, radix_bits)
+            off = offsets[c * F:(c + 1) * F]
+            p.prefix_sum(keys, c, num_chunks, off)
+            p.partition(keys, pays, c, num_chunks, off, rel)
+        except Exception as e:  # reported after the join
+            errors.append(e)
+
+    ts = [threading.Thread(target=run, args=(c,)) for c in range(num_chunks)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errors:
+        raise errors[0]
+    return rel, offsets
+
+
 class CudaRadixJoin:
     """CudaRadixJoin (cuda_radix_join.rs:116-164)."""
 

@@ -272,6 +272,57 @@ int fi_gpu_chunked_prefix_sum_noalloc_int64(const int64_t *partition_attr,
                                             uint64_t *offsets,
                                             fi_stream_t stream);
 
+/* ---- CpuRadixPartitioner (sql-ops/src/partition/cpu_radix_partition.rs:
+ *      25-560; kernels in sql-ops/cpputils/radix_partition.cpp) --------- */
+
+typedef enum {
+  FI_CPU_HISTOGRAM_CHUNKED = 0,
+  FI_CPU_HISTOGRAM_CHUNKED_SIMD = 1 /* same result as Chunked */
+} fi_cpu_histogram_algorithm;
+typedef enum {
+  FI_CPU_PARTITION_NC = 0,   /* one store per tuple at its partition cursor */
+  FI_CPU_PARTITION_SWWC = 1, /* software write-combining: 64-byte line buffers */
+  FI_CPU_PARTITION_SWWC_SIMD = 2 /* same as SWWC */
+} fi_cpu_partition_algorithm;
+
+typedef struct fi_cpu_radix_partitioner fi_cpu_radix_partitioner;
+
+/* A partitioner owns the per-thread state of one chunk at a time (its
+ * write-combining buffers): use one per thread, as the reference does.
+ * radix_bits <= 16.  Host only. */
+int fi_cpu_radix_partitioner_new(fi_cpu_histogram_algorithm histogram,
+                                 fi_cpu_partition_algorithm algorithm,
+                                 uint32_t radix_bits,
+                                 fi_cpu_radix_partitioner **out);
+void fi_cpu_radix_partitioner_free(fi_cpu_radix_partitioner *p);
+/* CpuRadixPartitioner::prefix_sum for chunk chunk_id of num_chunks (the
+ * canonical chunking of fi_input_chunk_size over data_len keys):
+ * chunk_offsets[0..F) receive the chunk's Chunked offsets, identical to
+ * fi_gpu_prefix_sum with Chunked at the same chunk count, i.e.
+ * offsets[c*F + p] of the whole relation. */
+int fi_cpu_prefix_sum_int32(fi_cpu_radix_partitioner *p, const int32_t *keys,
+                            uint64_t data_len, uint32_t chunk_id,
+                            uint32_t num_chunks, uint32_t ignore_bits,
+                            uint64_t *chunk_offsets);
+int fi_cpu_prefix_sum_int64(fi_cpu_radix_partitioner *p, const int64_t *keys,
+                            uint64_t data_len, uint32_t chunk_id,
+                            uint32_t num_chunks, uint32_t ignore_bits,
+                            uint64_t *chunk_offsets);
+/* CpuRadixPartitioner::partition for the same chunk: writes its tuples
+ * (AoS) into the relation (relation_len tuples, padded Chunked layout)
+ * from chunk_offsets, in input order within each partition; padding is not
+ * written.  Offsets that lead outside the relation are FI_ERR_CAPACITY. */
+int fi_cpu_partition_int32(fi_cpu_radix_partitioner *p, const int32_t *keys,
+                           const int32_t *pays, uint64_t data_len,
+                           uint32_t chunk_id, uint32_t num_chunks,
+                           uint32_t ignore_bits, const uint64_t *chunk_offsets,
+                           void *relation, uint64_t relation_len);
+int fi_cpu_partition_int64(fi_cpu_radix_partitioner *p, const int64_t *keys,
+                           const int64_t *pays, uint64_t data_len,
+                           uint32_t chunk_id, uint32_t num_chunks,
+                           uint32_t ignore_bits, const uint64_t *chunk_offsets,
+                           void *relation, uint64_t relation_len);
+
 /* ---- CudaRadixJoin (sql-ops/src/join/cuda_radix_join.rs:116-164) ------ */
 typedef struct fi_cuda_radix_join fi_cuda_radix_join;
 
