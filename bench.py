@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
-                    choices=["join", "partition", "ooc", "serve", "dataset", "nopart"],
+                    choices=["join", "partition", "ooc", "serve", "dataset", "nopart",
+                             "hybrid"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
                          "join server against back-to-back plain calls; dataset: "
@@ -72,6 +73,9 @@ def parse():
                          "data set's own")
     ap.add_argument("--selectivity", type=int, default=100,
                     help="dataset workload: join selectivity in percent")
+    ap.add_argument("--hybrid-log2n", type=int, default=28,
+                    help="hybrid join: |R| = |S| = 2^hybrid_log2n int64 tuples in "
+                         "host memory")
     ap.add_argument("--ht-scheme", default="linearprobing",
                     choices=["linearprobing", "perfect"],
                     help="nopart workload: hash table of the no-partitioning join")
@@ -1103,6 +1107,64 @@ def run_nopart(a):
         dist.destroy_process_group()
 
 
+def run_hybrid(a):
+    """Hybrid join (the reference's cpu_partitioned_radix_join): host
+    columns, first pass on all host threads, second pass and join on the GPU.
+    Wall-clock time per join (the CPU pass dominates); G tuples/s."""
+    import torch
+    import fi_sqlops as fi
+    world, rank, local = dist_setup(a.gpus)
+    n = 1 << a.hybrid_log2n
+    seed = a.seed + 1000 * rank
+    host = []
+    for gen in ("pk", "fk"):
+        d = torch.empty(n, dtype=torch.int64, device="cuda")
+        if gen == "pk":
+            fi.gen_primary_keys(d, seed, base=1)
+        else:
+            fi.gen_uniform_foreign_keys(d, n, seed + 1, base=1)
+            expected_sum = int(d.sum().item())
+        for _ in range(2):
+            h = torch.empty(n, dtype=torch.int64, pin_memory=True)
+            h.copy_(d)
+            host.append(h)
+        del d
+    torch.cuda.empty_cache()
+    threads = os.cpu_count() or 1
+    engine = fi.RadixJoinEngine(n, n, torch.int64, fi.RadixBits(9, 9),
+                                fi.HashingScheme.BucketChaining)
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        s, c = engine.run_hybrid(*host, threads=threads)
+        verified = verified and (c == n and s == expected_sum)
+    wall = []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            barrier(world)
+            t0 = time.perf_counter()
+            s, c = engine.run_hybrid(*host, threads=threads)
+            wall.append(time.perf_counter() - t0)
+            verified = verified and (c == n and s == expected_sum)
+    ms = max_over_ranks(statistics.mean(wall) * 1e3, world)
+    if rank == 0:
+        line = {"metric": "hybrid radix join G tuples/s",
+                "value": world * 2 * n / (ms / 1e3) / 1e9, "unit": UNIT,
+                "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded permutation PK, uniform FK, payload = key) "
+                        "in pinned host memory",
+                "config": {"workload": "hybrid_radix_join_%dMx%dM_int64_9+9bits"
+                                       % (n >> 20, n >> 20),
+                           "host_threads": threads, "timing": "wall clock per join",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "clocks": clk.summary(), "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -1117,6 +1179,8 @@ def main():
         run_dataset(a)
     elif a.workload == "nopart":
         run_nopart(a)
+    elif a.workload == "hybrid":
+        run_hybrid(a)
     else:
         run_ours(a)
 

@@ -26,6 +26,8 @@
 // Contiguous layout, as the join requires.
 #include <algorithm>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "../../include/fi_sqlops.h"
 #include "api_internal.h"
@@ -353,6 +355,10 @@ struct fi_radix_join_engine {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t slot_ready[2] = {}, slot_free[2] = {};
   DevBuf stage_key[2], stage_pay[2], stream_loc, result_dev;
+  // hybrid run: the CPU's first-pass relations and offsets in pinned memory
+  void *host_rel[2] = {nullptr, nullptr};
+  uint64_t *host_off[2] = {nullptr, nullptr};
+  size_t host_rel_bytes[2] = {0, 0};
   uint64_t workspace = 0;
   cudaEvent_t events[FI_ENGINE_PHASE_EVENTS] = {};
   bool record = false;
@@ -399,6 +405,13 @@ struct fi_radix_join_engine {
     }
     stream_loc.release();
     result_dev.release();
+    for (int i = 0; i < 2; ++i) {
+      if (host_rel[i]) cudaFreeHost(host_rel[i]);
+      if (host_off[i]) cudaFreeHost(host_off[i]);
+      host_rel[i] = nullptr;
+      host_off[i] = nullptr;
+      host_rel_bytes[i] = 0;
+    }
     if (copy_stream) cudaStreamDestroy(copy_stream);
     copy_stream = nullptr;
   }
@@ -1020,6 +1033,122 @@ static int engine_run_streamed(fi_radix_join_engine *e, const K *bk,
         "result copy");
   FI_CK(cudaStreamSynchronize(st), "synchronize");
   return FI_OK;
+}
+
+// Hybrid join (radix-join/src/execution_methods/cpu_partitioned_radix_join.rs:
+// 118-769): the first pass runs on the CPU, one canonical chunk per host
+// thread (cpu_partition.cu, write-combining scatter) into pinned memory; the
+// partitioned relation and its Chunked offsets are copied to the device and
+// the GPU runs the second pass and the join.  The CPU partitions S while
+// the GPU copies R and runs its second pass.  Synchronous.
+template <typename K>
+static int engine_run_hybrid(fi_radix_join_engine *e, const K *bk, const K *bp,
+                             uint64_t bn, const K *pk, const K *pp, uint64_t pn,
+                             uint32_t threads, fi_join_result *result,
+                             cudaStream_t st) {
+  int rc = engine_check<K>(e, 0, bk, bp, bn);
+  if (!rc) rc = engine_check<K>(e, 1, pk, pp, pn);
+  if (rc) return rc;
+  if (!result) return set_error(FI_ERR_INVALID_ARGUMENT, "null result");
+  if (e->bits2 < 0)
+    return set_error(FI_ERR_UNSUPPORTED,
+                     "the hybrid join runs the second pass on the GPU; it needs "
+                     "two radix passes");
+  if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t C = std::min(threads, e->C1);
+  const uint32_t F1 = e->F1, b1 = (uint32_t)e->bits1;
+  const uint64_t pad = kPaddingBytes / sizeof(Tuple<K>);
+  const uint64_t lens[2] = {bn, pn};
+  const K *keys[2] = {bk, pk}, *pays[2] = {bp, pp};
+  for (int r = 0; r < 2; ++r) {
+    const size_t need = (size_t)(lens[r] + (uint64_t)C * F1 * pad) * sizeof(Tuple<K>);
+    if (e->host_rel_bytes[r] < need) {
+      if (e->host_rel[r]) cudaFreeHost(e->host_rel[r]);
+      e->host_rel[r] = nullptr;
+      e->host_rel_bytes[r] = 0;
+      FI_CK(cudaHostAlloc(&e->host_rel[r], need, cudaHostAllocDefault),
+            "pinned host relation");
+      e->host_rel_bytes[r] = need;
+    }
+    if (!e->host_off[r])
+      FI_CK(cudaHostAlloc((void **)&e->host_off[r], (size_t)e->C1 * e->F1 * 8,
+                          cudaHostAllocDefault),
+            "pinned host offsets");
+  }
+  e->launches = 0;
+  e->mark(0, st);
+  for (int r = 0; r < 2; ++r) {
+    const uint64_t padded1 = lens[r] + (uint64_t)C * F1 * pad;
+    // R's copy may still be running while S is partitioned: each relation
+    // has its own pinned buffer
+    std::vector<int> rcs(C, FI_OK);
+    std::vector<std::thread> pool;
+    pool.reserve(C);
+    for (uint32_t c = 0; c < C; ++c)
+      pool.emplace_back([&, c]() {
+        fi_cpu_radix_partitioner *p = nullptr;
+        int x = fi_cpu_radix_partitioner_new(FI_CPU_HISTOGRAM_CHUNKED,
+                                             FI_CPU_PARTITION_SWWC, b1, &p);
+        uint64_t *off = e->host_off[r] + (size_t)c * F1;
+        if (!x)
+          x = sizeof(K) == 4
+                  ? fi_cpu_prefix_sum_int32(p, (const int32_t *)keys[r], lens[r], c, C, 0, off)
+                  : fi_cpu_prefix_sum_int64(p, (const int64_t *)keys[r], lens[r], c, C, 0, off);
+        if (!x)
+          x = sizeof(K) == 4
+                  ? fi_cpu_partition_int32(p, (const int32_t *)keys[r],
+                                           (const int32_t *)pays[r], lens[r], c, C, 0,
+                                           off, e->host_rel[r], padded1)
+                  : fi_cpu_partition_int64(p, (const int64_t *)keys[r],
+                                           (const int64_t *)pays[r], lens[r], c, C, 0,
+                                           off, e->host_rel[r], padded1);
+        fi_cpu_radix_partitioner_free(p);
+        rcs[c] = x;
+      });
+    for (auto &t : pool) t.join();
+    for (uint32_t c = 0; c < C; ++c)
+      if (rcs[c]) return set_error(rcs[c], "CPU first pass of relation %d failed", r);
+    e->mark(1 + 4 * r, st);
+    FI_CK(cudaMemcpyAsync(e->off1[r].ptr, e->host_off[r], (size_t)C * F1 * 8,
+                          cudaMemcpyHostToDevice, st),
+          "offsets copy");
+    FI_CK(cudaMemcpyAsync(e->rel1[r].ptr, e->host_rel[r],
+                          (size_t)padded1 * sizeof(Tuple<K>), cudaMemcpyHostToDevice, st),
+          "relation copy");
+    e->mark(2 + 4 * r, st);
+    rc = engine_pass2<K>(e, r, C, padded1, lens[r], st);
+    if (rc) return rc;
+    e->part_len[r] = lens[r];
+  }
+  e->built = true;
+  rc = e->result_dev.reserve(sizeof(fi_join_result), false);
+  if (rc) return rc;
+  rc = engine_join<K>(e, (fi_join_result *)e->result_dev.ptr, st);
+  if (rc) return rc;
+  FI_CK(cudaMemcpyAsync(result, e->result_dev.ptr, sizeof(fi_join_result),
+                        cudaMemcpyDeviceToHost, st),
+        "result copy");
+  FI_CK(cudaStreamSynchronize(st), "synchronize");
+  return FI_OK;
+}
+
+extern "C" int fi_radix_join_engine_run_hybrid_int32(
+    fi_radix_join_engine *e, const int32_t *build_key, const int32_t *build_pay,
+    uint64_t build_len, const int32_t *probe_key, const int32_t *probe_pay,
+    uint64_t probe_len, uint32_t threads, fi_join_result *result,
+    fi_stream_t stream) {
+  return engine_run_hybrid<int32_t>(e, build_key, build_pay, build_len, probe_key,
+                                    probe_pay, probe_len, threads, result,
+                                    (cudaStream_t)stream);
+}
+extern "C" int fi_radix_join_engine_run_hybrid_int64(
+    fi_radix_join_engine *e, const int64_t *build_key, const int64_t *build_pay,
+    uint64_t build_len, const int64_t *probe_key, const int64_t *probe_pay,
+    uint64_t probe_len, uint32_t threads, fi_join_result *result,
+    fi_stream_t stream) {
+  return engine_run_hybrid<int64_t>(e, build_key, build_pay, build_len, probe_key,
+                                    probe_pay, probe_len, threads, result,
+                                    (cudaStream_t)stream);
 }
 
 extern "C" int fi_radix_join_engine_run_streamed_int32(

@@ -38,6 +38,8 @@
 //    flight and each item waits on its first chunks; bulk L2 prefetches of
 //    the next item's build and probe ranges: 10.37 ms; eight probe loads in
 //    flight per thread instead of four: 9.16 ms (register spills).
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -219,12 +221,97 @@ __host__ __device__ inline uint32_t chain_capacity(uint32_t table_bytes,
   return cap < 65528u ? cap : 65528u;
 }
 
+// Heavy partitions (bucket chaining): a partition whose build side exceeds
+// the table was left out of the items and listed at the end of item_part;
+// each becomes R x Q units (build round r of `cap` tuples x probe slice q of
+// at most `width` tuples), numbered consecutively over the list and dealt
+// round-robin to the CTAs.  A partition of tens of millions of equal build
+// keys (e.g. the null keys of a selective data set) is so spread over the
+// whole GPU instead of being joined round after round by one CTA.  Called
+// by every thread of radix_join_kernel after its items, with the CTA's table
+// in `smem`; kept out of line so that the item loop's code is the same with
+// and without it (inlined, the kernel's register allocation changed and the
+// join of 1024M x 1024M int64 became 4% slower).
+struct HeavyResult {
+  int64_t sum;
+  uint64_t cnt;
+};
+
+template <typename K>
+__device__ __noinline__ HeavyResult join_heavy_units(
+    unsigned char *smem, const Tuple<K> *__restrict__ build,
+    const uint64_t *__restrict__ build_off, uint64_t build_len, uint32_t build_pad,
+    const Tuple<K> *__restrict__ probe, const uint64_t *__restrict__ probe_off,
+    uint64_t probe_len, uint32_t probe_pad, uint32_t F, uint32_t ignore_bits,
+    const uint32_t *__restrict__ item_part, uint32_t item_cap, uint32_t H,
+    uint32_t width, uint32_t table_bytes, uint32_t log2_buckets) {
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t cap = chain_capacity<K>(table_bytes, log2_buckets);
+  K *tkeys = reinterpret_cast<K *>(smem);
+  uint16_t *tnext = reinterpret_cast<uint16_t *>(tkeys + cap);
+  uint32_t *heads =
+      reinterpret_cast<uint32_t *>(smem + ((cap * (sizeof(K) + 2) + 15) & ~15u));
+  const uint32_t nbuckets = 1u << log2_buckets;
+  HeavyResult res{0, 0};
+  int64_t cached_p = -1, cached_r = -1;
+  uint64_t g0 = 0;
+  for (uint32_t h = 0; h < H; ++h) {
+    const uint32_t hp = item_part[item_cap - 1u - h];
+    uint64_t bb, be, pb, pe;
+    part_bounds(build_off, build_len, build_pad, F, hp, bb, be);
+    part_bounds(probe_off, probe_len, probe_pad, F, hp, pb, pe);
+    const uint64_t bsize = be - bb, psize = pe - pb;
+    const uint64_t R = (bsize + cap - 1) / cap;
+    const uint64_t Q = (psize + width - 1) / width;
+    const uint64_t per = (psize + Q - 1) / Q;
+    const uint64_t U = R * Q;
+    uint64_t g = g0 + (blockIdx.x + gridDim.x - g0 % gridDim.x) % gridDim.x;
+    for (; g < g0 + U; g += gridDim.x) {
+      const uint64_t u = g - g0, r = u / Q, qi = u % Q;
+      if (!(cached_p == (int64_t)hp && cached_r == (int64_t)r)) {
+        const uint64_t r0 = r * cap;
+        const uint32_t rn = (uint32_t)min((uint64_t)cap, bsize - r0);
+        __syncthreads();  // the previous unit's probe is done with the table
+        for (uint32_t i = tid; i < nbuckets; i += nt) heads[i] = kHeadEnd;
+        __syncthreads();
+        for (uint32_t i = tid; i < rn; i += nt) {
+          const K key = build[bb + r0 + i].key;
+          tkeys[i] = key;
+          const uint32_t old =
+              atomicExch(&heads[chain_bucket(key, ignore_bits, log2_buckets)], i);
+          tnext[i] = (uint16_t)(old == kHeadEnd ? kLinkEnd : old);
+        }
+        __syncthreads();
+        cached_p = hp;
+        cached_r = (int64_t)r;
+      }
+      const uint64_t qb = min(pe, pb + per * qi), qe = min(pe, qb + per);
+      for (uint64_t j = qb + tid; j < qe; j += nt) {
+        const Tuple<K> t = load_tuple_cs(probe + j);
+        uint32_t e = heads[chain_bucket(t.key, ignore_bits, log2_buckets)];
+        if (e == kHeadEnd) continue;
+        for (;;) {
+          if (tkeys[e] == t.key) {
+            res.sum += static_cast<int64_t>(t.value);
+            res.cnt += 1;
+          }
+          const uint32_t nx = tnext[e];
+          if (nx == kLinkEnd) break;
+          e = nx;
+        }
+      }
+    }
+    g0 += U;
+  }
+  return res;
+}
+
 // Persistent join: CTA b takes items b, b + grid, b + 2*grid, ...  Items
 // are near-equal in probe work (at most `width` probe tuples each), so the
 // grid stride balances skewed inputs while avoiding a global work counter;
 // the partition of the next item is prefetched.  With bucket chaining the
 // planner gives no items to partitions whose build side exceeds the table;
-// radix_join_heavy_kernel joins those.
+// join_heavy_units joins those after the items.
 template <typename K, int kScheme, int kMaxThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
     const Tuple<K> *__restrict__ build, const uint64_t *__restrict__ build_off,
@@ -234,7 +321,8 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
     const uint32_t *__restrict__ item_start,
     const uint32_t *__restrict__ item_part, uint32_t table_bytes,
     uint32_t log2_buckets, int64_t *__restrict__ result_set,
-    uint64_t *match_count, int *status) {
+    uint64_t *match_count, int *status, uint32_t item_cap,
+    const uint32_t *__restrict__ heavy_count, uint32_t width) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t s_used;
   __shared__ uint64_t red_tmp[32];
@@ -361,97 +449,18 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
     }
     p = np;
   }
-
-  result_set[(uint64_t)blockIdx.x * nt + tid] += sum;
-  if (match_count != nullptr) {
-    const uint64_t bc = block_reduce_u64(cnt, red_tmp);
-    if (tid == 0 && bc != 0)
-      atomicAdd((unsigned long long *)match_count, (unsigned long long)bc);
-  }
-}
-
-// Heavy partitions (bucket chaining): a partition whose build side exceeds
-// the table was left out of the items and listed at the end of item_part;
-// each becomes R x Q units (build round r of `cap` tuples x probe slice q of
-// at most `width` tuples), numbered consecutively over the list and dealt
-// round-robin to the CTAs.  A partition of tens of millions of equal build
-// keys (e.g. the null keys of a selective data set) is so spread over the
-// whole GPU instead of being joined round after round by one CTA.  Same
-// table layout, launch shape and result slots as radix_join_kernel; with
-// no heavy partition every CTA returns at once.
-template <typename K, int kMaxThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_heavy_kernel(
-    const Tuple<K> *__restrict__ build, const uint64_t *__restrict__ build_off,
-    uint64_t build_len, uint32_t build_pad, const Tuple<K> *__restrict__ probe,
-    const uint64_t *__restrict__ probe_off, uint64_t probe_len,
-    uint32_t probe_pad, uint32_t F, uint32_t ignore_bits,
-    const uint32_t *__restrict__ item_part, uint32_t item_cap,
-    const uint32_t *__restrict__ heavy_count, uint32_t width,
-    uint32_t table_bytes, uint32_t log2_buckets,
-    int64_t *__restrict__ result_set, uint64_t *match_count) {
-  const uint32_t H = *heavy_count;
-  if (H == 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint64_t red_tmp[32];
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
-  const uint32_t cap = chain_capacity<K>(table_bytes, log2_buckets);
-  K *tkeys = reinterpret_cast<K *>(smem_raw);
-  uint16_t *tnext = reinterpret_cast<uint16_t *>(tkeys + cap);
-  uint32_t *heads =
-      reinterpret_cast<uint32_t *>(smem_raw + ((cap * (sizeof(K) + 2) + 15) & ~15u));
-  const uint32_t nbuckets = 1u << log2_buckets;
-  int64_t sum = 0;
-  uint64_t cnt = 0;
-  int64_t cached_p = -1, cached_r = -1;
-  uint64_t g0 = 0;
-  for (uint32_t h = 0; h < H; ++h) {
-    const uint32_t hp = item_part[item_cap - 1u - h];
-    uint64_t bb, be, pb, pe;
-    part_bounds(build_off, build_len, build_pad, F, hp, bb, be);
-    part_bounds(probe_off, probe_len, probe_pad, F, hp, pb, pe);
-    const uint64_t bsize = be - bb, psize = pe - pb;
-    const uint64_t R = (bsize + cap - 1) / cap;
-    const uint64_t Q = (psize + width - 1) / width;
-    const uint64_t per = (psize + Q - 1) / Q;
-    const uint64_t U = R * Q;
-    uint64_t g = g0 + (blockIdx.x + gridDim.x - g0 % gridDim.x) % gridDim.x;
-    for (; g < g0 + U; g += gridDim.x) {
-      const uint64_t u = g - g0, r = u / Q, qi = u % Q;
-      if (!(cached_p == (int64_t)hp && cached_r == (int64_t)r)) {
-        const uint64_t r0 = r * cap;
-        const uint32_t rn = (uint32_t)min((uint64_t)cap, bsize - r0);
-        __syncthreads();  // the previous unit's probe is done with the table
-        for (uint32_t i = tid; i < nbuckets; i += nt) heads[i] = kHeadEnd;
-        __syncthreads();
-        for (uint32_t i = tid; i < rn; i += nt) {
-          const K key = build[bb + r0 + i].key;
-          tkeys[i] = key;
-          const uint32_t old =
-              atomicExch(&heads[chain_bucket(key, ignore_bits, log2_buckets)], i);
-          tnext[i] = (uint16_t)(old == kHeadEnd ? kLinkEnd : old);
-        }
-        __syncthreads();
-        cached_p = hp;
-        cached_r = (int64_t)r;
-      }
-      const uint64_t qb = min(pe, pb + per * qi), qe = min(pe, qb + per);
-      for (uint64_t j = qb + tid; j < qe; j += nt) {
-        const Tuple<K> t = load_tuple_cs(probe + j);
-        uint32_t e = heads[chain_bucket(t.key, ignore_bits, log2_buckets)];
-        if (e == kHeadEnd) continue;
-        for (;;) {
-          if (tkeys[e] == t.key) {
-            sum += static_cast<int64_t>(t.value);
-            cnt += 1;
-          }
-          const uint32_t nx = tnext[e];
-          if (nx == kLinkEnd) break;
-          e = nx;
-        }
-      }
+  if (kScheme == 2 && heavy_count != nullptr) {
+    const uint32_t H = *heavy_count;
+    if (H) {
+      const HeavyResult hr = join_heavy_units<K>(
+          smem_raw, build, build_off, build_len, build_pad, probe, probe_off,
+          probe_len, probe_pad, F, ignore_bits, item_part, item_cap, H, width,
+          table_bytes, log2_buckets);
+      sum += hr.sum;
+      cnt += hr.cnt;
     }
-    g0 += U;
   }
+
   result_set[(uint64_t)blockIdx.x * nt + tid] += sum;
   if (match_count != nullptr) {
     const uint64_t bc = block_reduce_u64(cnt, red_tmp);
@@ -488,9 +497,24 @@ uint32_t join_ctas_per_sm(uint32_t block) {
   return block <= 256 ? 4u : block <= 512 ? 2u : 1u;
 }
 
-// Dynamic shared memory of one join CTA when `ctas` share an SM.
+template <typename K, int kScheme>
+static uint32_t join_dyn_smem_query(uint32_t ctas);
+
+// Dynamic shared memory of one join CTA when `ctas` share an SM (queried
+// once per kernel and shape; every device of a process is taken to be a B200).
 template <typename K, int kScheme>
 static uint32_t join_dyn_smem(uint32_t ctas) {
+  static std::atomic<uint32_t> cached[3];
+  const int slot = ctas == 4 ? 0 : ctas == 2 ? 1 : 2;
+  const uint32_t c = cached[slot].load(std::memory_order_relaxed);
+  if (c) return c;
+  const uint32_t v = join_dyn_smem_query<K, kScheme>(ctas);
+  cached[slot].store(v, std::memory_order_relaxed);
+  return v;
+}
+
+template <typename K, int kScheme>
+static uint32_t join_dyn_smem_query(uint32_t ctas) {
   cudaFuncAttributes attr;
   if (cudaFuncGetAttributes(&attr, join_kernel_ptr<K, kScheme>(ctas)) != cudaSuccess) {
     cudaGetLastError();
@@ -598,33 +622,16 @@ cudaError_t launch_radix_join(const void *build, const uint64_t *build_off,
   radix_join_kernel<K, S, T, M><<<grid, block, dyn, stream>>>(                 \
       b, build_off, build_len, build_pad, pr, probe_off, probe_len, probe_pad, \
       fanout, ignore_bits, s.item_start, s.item_part, dyn, lb, result_set,     \
-      match_count, s.status)
-#define FI_HEAVY_LAUNCH(T, M)                                                   \
-  do {                                                                          \
-    e = cudaFuncSetAttribute((const void *)radix_join_heavy_kernel<K, T, M>,    \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,       \
-                             (int)dyn);                                         \
-    if (e != cudaSuccess) return e;                                             \
-    radix_join_heavy_kernel<K, T, M><<<grid, block, dyn, stream>>>(             \
-        b, build_off, build_len, build_pad, pr, probe_off, probe_len,           \
-        probe_pad, fanout, ignore_bits, s.item_part, item_cap, heavy_count,     \
-        (uint32_t)width, dyn, lb, result_set, match_count);                     \
-  } while (0)
+      match_count, s.status, item_cap, heavy_count, (uint32_t)width)
   if (scheme == 2) {
     if (ctas == 4) FI_JOIN_LAUNCH(2, 256, 4);
     else if (ctas == 2) FI_JOIN_LAUNCH(2, 512, 2);
     else FI_JOIN_LAUNCH(2, 1024, 1);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (ctas == 4) FI_HEAVY_LAUNCH(256, 4);
-    else if (ctas == 2) FI_HEAVY_LAUNCH(512, 2);
-    else FI_HEAVY_LAUNCH(1024, 1);
   } else {
     if (ctas == 4) FI_JOIN_LAUNCH(0, 256, 4);
     else if (ctas == 2) FI_JOIN_LAUNCH(0, 512, 2);
     else FI_JOIN_LAUNCH(0, 1024, 1);
   }
-#undef FI_HEAVY_LAUNCH
 #undef FI_JOIN_LAUNCH
   return cudaGetLastError();
 }

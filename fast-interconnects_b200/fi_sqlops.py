@@ -609,6 +609,18 @@ class RadixJoinEngine:
             C.c_uint64(probe_key.numel()), C.byref(res), _stream(stream)))
         return res.sum, res.count
 
+    def run_hybrid(self, build_key, build_pay, probe_key, probe_pay, threads=0,
+                   stream=None):
+        """Hybrid join: host columns in; the first pass on `threads` host
+        threads (0 = all), the second pass and the join on the GPU;
+        (sum, count) out; synchronous."""
+        res = _JoinResultC()
+        f = getattr(lib(), "fi_radix_join_engine_run_hybrid_" + _sfx(build_key.dtype))
+        _check(f(self.h, _ptr(build_key), _ptr(build_pay), C.c_uint64(build_key.numel()),
+                 _ptr(probe_key), _ptr(probe_pay), C.c_uint64(probe_key.numel()),
+                 C.c_uint32(threads), C.byref(res), _stream(stream)))
+        return res.sum, res.count
+
     def set_plan(self, radix_bits, hashing_scheme=HashingScheme.BucketChaining,
                  join_block=0, scatter=0):
         """Plan of the following runs, within the engine's creation bits

@@ -463,6 +463,32 @@ int fi_radix_join_engine_probe_int64(fi_radix_join_engine *e,
                                      fi_join_result *result,
                                      fi_stream_t stream);
 
+/* Hybrid join (cpu_partitioned_radix_join.rs:118-769): host columns in,
+ * (sum, count) out.  The first pass runs on the CPU (threads host threads,
+ * one canonical chunk each, 0 = all hardware threads, at most the engine's
+ * chunk count) into the engine's pinned host buffers; the partitioned
+ * relations and their Chunked offsets are copied to the device, and the
+ * GPU runs the second pass and the join.  The CPU partitions S while the GPU
+ * copies and partitions R.  Needs a two-pass plan.  Synchronous. */
+int fi_radix_join_engine_run_hybrid_int32(fi_radix_join_engine *e,
+                                          const int32_t *build_key,
+                                          const int32_t *build_pay,
+                                          uint64_t build_len,
+                                          const int32_t *probe_key,
+                                          const int32_t *probe_pay,
+                                          uint64_t probe_len, uint32_t threads,
+                                          fi_join_result *result,
+                                          fi_stream_t stream);
+int fi_radix_join_engine_run_hybrid_int64(fi_radix_join_engine *e,
+                                          const int64_t *build_key,
+                                          const int64_t *build_pay,
+                                          uint64_t build_len,
+                                          const int64_t *probe_key,
+                                          const int64_t *probe_pay,
+                                          uint64_t probe_len, uint32_t threads,
+                                          fi_join_result *result,
+                                          fi_stream_t stream);
+
 /* Out-of-core join (no reference counterpart; the nearest reference pieces
  * are the chunked multi-stream copy of numa-gpu/src/runtime/cuda.rs:891-985
  * and the cache-and-spill staging of gpu_triton_join.rs:391-470).  The four
