@@ -138,6 +138,19 @@ __device__ __forceinline__ uint32_t warp_aggregated_rank(uint32_t *counters,
   return rank;
 }
 
+// Rank with one shared atomic per warp when all 32 lanes are active and
+// share one bin (a tile inside a Zipf-hot partition), else one per lane.
+__device__ __forceinline__ uint32_t warp_uniform_rank(uint32_t *counters,
+                                                      uint32_t bin, bool active) {
+  const uint32_t b0 = __shfl_sync(kFullMask, bin, 0);
+  if (__all_sync(kFullMask, active && bin == b0)) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(&counters[bin], 32u);
+    return __shfl_sync(kFullMask, base, 0) + lane_id();
+  }
+  return active ? atomicAdd(&counters[bin], 1u) : 0u;
+}
+
 // Same as warp_aggregated_rank without a result (histograms).
 __device__ __forceinline__ void warp_aggregated_count(uint32_t *counters,
                                                       uint32_t bin,

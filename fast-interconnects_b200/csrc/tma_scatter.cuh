@@ -203,7 +203,7 @@ struct TmaRegionSource {
 // so no separate staging buffer is needed and the stages can be 50% longer.
 // Called once per barrier initialisation by all threads; thread 0 issues
 // the copies.
-template <typename K, typename Src>
+template <typename K, typename Src, bool kUniformWarps = false>
 __device__ __forceinline__ void tma_tile_scatter_range(
     Src &src, uint64_t begin, uint64_t end, uint32_t F, uint64_t mask,
     uint32_t ignore_bits, uint32_t *cur, uint32_t *toff, uint32_t *warp_tmp,
@@ -246,7 +246,8 @@ __device__ __forceinline__ void tma_tile_scatter_range(
       const bool act = ok && i < n_valid;
       if (act) src.get(stage, t0, n_valid, i, ck[u], cv[u]);
       pp[u] = act ? key_to_partition(ck[u], mask, ignore_bits) : 0u;
-      rk[u] = warp_aggregated_rank(toff, pp[u], act);
+      rk[u] = kUniformWarps ? warp_uniform_rank(toff, pp[u], act)
+                            : warp_aggregated_rank(toff, pp[u], act);
     }
     // barrier 1: every tuple of the stage is in registers; also the vote on
     // a wait that gave up
