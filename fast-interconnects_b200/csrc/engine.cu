@@ -137,7 +137,12 @@ __device__ __forceinline__ uint32_t find_p1(const uint32_t *piece_first,
   return lo;
 }
 
-// Histogram of piece k on the second-pass bits.
+// Histogram of piece k on the second-pass bits.  It reads the whole pass-1
+// tuples for their keys (16 bytes per tuple).  Measured on B200 and left
+// out: pass 1 storing each tuple's second-pass digit as a u16 beside the
+// tuple, for this histogram to read 2 bytes per tuple: the histogram went
+// from 2.9 to 2.0 ms per relation (1024M int64), but the digit stores, two
+// bytes each in short runs, made the pass-1 scatter 6.97 -> 12.0 ms.
 template <typename K>
 __global__ void __launch_bounds__(512)
     piece_histogram_kernel(const Tuple<K> *__restrict__ rel1,
