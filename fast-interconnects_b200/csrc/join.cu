@@ -37,7 +37,10 @@
 //    buffers): 9.63 ms, since 227 KB cannot keep a whole next partition in
 //    flight and each item waits on its first chunks; bulk L2 prefetches of
 //    the next item's build and probe ranges: 10.37 ms; eight probe loads in
-//    flight per thread instead of four: 9.16 ms (register spills).
+//    flight per thread instead of four: 9.16 ms (register spills), or 8.20
+//    ms with three 256-thread CTAs per SM to give them the registers: the
+//    number of partitions an SM works on at once matters more than the
+//    loads each thread keeps in flight.
 #include <atomic>
 
 #include "common.cuh"
