@@ -67,6 +67,7 @@ def lib():
         _lib.fi_padding_len.restype = C.c_uint32
         _lib.fi_partitioned_relation_alloc_len.restype = C.c_uint64
         _lib.fi_radix_join_engine_workspace_bytes.restype = C.c_uint64
+        _lib.fi_gpu_prefix_sum_state_len.restype = C.c_uint64
         # the autotuner's measured table (autotune.py), when it exists
         if os.path.exists(TUNING_TABLE):
             _check(_lib.fi_autotune_load(TUNING_TABLE.encode()))
@@ -377,6 +378,34 @@ class GpuRadixPartitioner:
 # ---------------------------------------------------------------------------
 # CudaRadixJoin
 # ---------------------------------------------------------------------------
+def prefix_sum_state_len(grid_size, block_size):
+    """GpuPrefixSum::state_len: scan-state entries (32 bytes each)."""
+    return lib().fi_gpu_prefix_sum_state_len(C.c_uint32(grid_size), C.c_uint32(block_size))
+
+
+def block_exclusive_prefix_sum(data, padding, grid_size, block_size, stream=None):
+    """host_block_exclusive_prefix_sum_uint64 on a device u64 (int64) tensor,
+    in place: each block scans its len/grid_size items."""
+    _check(lib().fi_block_exclusive_prefix_sum_uint64(
+        _ptr(data), C.c_uint64(data.numel()), C.c_uint64(padding),
+        C.c_uint32(grid_size), C.c_uint32(block_size), _stream(stream)))
+
+
+def device_exclusive_prefix_sum(data, padding, grid_size, block_size, stream=None):
+    """host_device_exclusive_prefix_sum[_initialize]_uint64 on a device u64
+    (int64) tensor, in place, with freshly initialised state."""
+    n = prefix_sum_state_len(grid_size, block_size)
+    state = torch.empty(4 * n, dtype=torch.int64, device=data.device)
+    status = torch.zeros(1, dtype=torch.int32, device=data.device)
+    _check(lib().fi_device_exclusive_prefix_sum_initialize_uint64(
+        _ptr(state), C.c_uint32(grid_size), C.c_uint32(block_size), _stream(stream)))
+    _check(lib().fi_device_exclusive_prefix_sum_uint64(
+        _ptr(data), C.c_uint64(data.numel()), C.c_uint64(padding), _ptr(state),
+        C.c_uint32(grid_size), C.c_uint32(block_size), _ptr(status), _stream(stream)))
+    if int(status.item()) != 0:
+        _check(int(status.item()))
+
+
 class CpuHistogramAlgorithm(enum.IntEnum):
     Chunked = 0
     ChunkedSimd = 1

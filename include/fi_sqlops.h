@@ -272,6 +272,33 @@ int fi_gpu_chunked_prefix_sum_noalloc_int64(const int64_t *partition_attr,
                                             uint64_t *offsets,
                                             fi_stream_t stream);
 
+/* ---- prefix scans of u64 arrays (the reference's scan test exports,
+ *      sql-ops/include/prefix_scan.h:55-122,213-384) -------------------- */
+
+/* GpuPrefixSum::state_len (sql-ops/src/prefix_scan/gpu_prefix_scan.rs:
+ * 40-51): entries of 32 bytes of scan state for a grid x block launch. */
+uint64_t fi_gpu_prefix_sum_state_len(uint32_t grid_size, uint32_t block_size);
+/* host_block_exclusive_prefix_sum_uint64: each of grid_size blocks scans its
+ * size/grid_size items in place; thread t of a block owns ceil(items /
+ * block_size) consecutive items and adds (t+1) * padding to each. */
+int fi_block_exclusive_prefix_sum_uint64(uint64_t *data, uint64_t size,
+                                         uint64_t padding, uint32_t grid_size,
+                                         uint32_t block_size, fi_stream_t stream);
+/* host_device_exclusive_prefix_sum_initialize_uint64 and
+ * host_device_exclusive_prefix_sum_uint64: a scan of the whole array over
+ * the grid, with state (fi_gpu_prefix_sum_state_len entries of 32 bytes)
+ * initialised before every scan; thread g of the grid owns ceil(size /
+ * threads) consecutive items and adds (g+1) * padding.  A look-back that
+ * waits too long records FI_ERR_TIMEOUT in *status (may be null). */
+int fi_device_exclusive_prefix_sum_initialize_uint64(void *state,
+                                                     uint32_t grid_size,
+                                                     uint32_t block_size,
+                                                     fi_stream_t stream);
+int fi_device_exclusive_prefix_sum_uint64(uint64_t *data, uint64_t size,
+                                          uint64_t padding, void *state,
+                                          uint32_t grid_size, uint32_t block_size,
+                                          int *status, fi_stream_t stream);
+
 /* ---- CpuRadixPartitioner (sql-ops/src/partition/cpu_radix_partition.rs:
  *      25-560; kernels in sql-ops/cpputils/radix_partition.cpp) --------- */
 
