@@ -569,6 +569,114 @@ class CudaHashJoin:
                  C.c_uint64(result_set.numel()), _stream(stream)))
 
 
+class CpuHashTable:
+    """HashTable::new_on_cpu (no_partitioning_join.rs:568-581): `mem_len`
+    host entries of {key, value} (a (mem_len, 2) numpy array of the key
+    type) whose keys are the null key; `size` is the size used for hashing."""
+
+    def __init__(self, size, dtype, mem_len=None):
+        import numpy as np
+        mem_len = size if mem_len is None else mem_len
+        if mem_len < size:
+            raise SqlOpsError(-1, "Provided memory must be larger than hash table size")
+        self.dtype = np.dtype(dtype)
+        self.size = size
+        self.mem = np.empty((max(mem_len, 1), 2), self.dtype)
+        f = getattr(lib(), "fi_cpu_hash_table_init_" + _cpu_sfx(self.mem))
+        _check(f(C.c_void_p(self.mem.ctypes.data), C.c_uint64(mem_len)))
+        self.mem_len = mem_len
+
+
+def _cpu_sfx(a):
+    import numpy as np
+    return "int32" if a.dtype == np.int32 else "int64"
+
+
+class CpuHashJoin:
+    """CpuHashJoin built like CpuHashJoinBuilder (no_partitioning_join.rs:
+    153-304, 740-772): build and probe_sum of numpy columns on the host.
+    Several threads may build (or probe) disjoint slices through one join."""
+
+    def __init__(self, hashing_scheme, hash_table, is_selective=False):
+        self.ht = hash_table
+        self.h = C.c_void_p()
+        _check(lib().fi_cpu_hash_join_new(
+            C.c_int(int(hashing_scheme)), C.c_int(1 if is_selective else 0),
+            C.c_void_p(hash_table.mem.ctypes.data), C.c_uint64(hash_table.mem_len),
+            C.c_uint64(hash_table.size), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fi_cpu_hash_join_free(self.h)
+            self.h = None
+
+    def _cols(self, join_attr, payload_attr):
+        import numpy as np
+        if len(join_attr) != len(payload_attr):
+            raise SqlOpsError(-1, "Join and payload attributes have different sizes")
+        if join_attr.dtype != self.ht.dtype or payload_attr.dtype != self.ht.dtype:
+            raise SqlOpsError(-1, "attributes must have the hash table's key type")
+        return (np.ascontiguousarray(join_attr), np.ascontiguousarray(payload_attr))
+
+    def build(self, join_attr, payload_attr):
+        k, p = self._cols(join_attr, payload_attr)
+        f = getattr(lib(), "fi_cpu_hash_join_build_" + _cpu_sfx(k))
+        _check(f(self.h, C.c_void_p(k.ctypes.data), C.c_void_p(p.ctypes.data),
+                 C.c_uint64(len(k))))
+
+    def probe_sum(self, join_attr, payload_attr, join_result=0):
+        """Returns join_result plus (wrapping mod 2^64) the payloads of all
+        matching probe tuples."""
+        k, p = self._cols(join_attr, payload_attr)
+        f = getattr(lib(), "fi_cpu_hash_join_probe_sum_" + _cpu_sfx(k))
+        acc = C.c_uint64(int(join_result) & 0xFFFFFFFFFFFFFFFF)
+        _check(f(self.h, C.c_void_p(k.ctypes.data), C.c_void_p(p.ctypes.data),
+                 C.c_uint64(len(k)), C.byref(acc)))
+        return acc.value
+
+
+def cpu_hash_join_sum(build_key, build_pay, probe_key, probe_pay, hashing_scheme,
+                      size, threads=1, is_selective=False, mem_len=None):
+    """Whole no-partitioning join on `threads` host threads, as the
+    reference's cpu_hash_join benchmark runs it: the threads build disjoint
+    slices into one shared table, then probe disjoint slices; returns the
+    u64 sum of the matched probe payloads."""
+    import threading
+    ht = CpuHashTable(size, build_key.dtype, mem_len)
+    hj = CpuHashJoin(hashing_scheme, ht, is_selective)
+    sums, errors = [0] * threads, []
+
+    def slices(n):
+        return [(n * t // threads, n * (t + 1) // threads) for t in range(threads)]
+
+    def run(fn):
+        ts = [threading.Thread(target=fn, args=(t,)) for t in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    def build(t):
+        try:
+            b, e = slices(len(build_key))[t]
+            hj.build(build_key[b:e], build_pay[b:e])
+        except Exception as ex:  # reported after the join
+            errors.append(ex)
+
+    def probe(t):
+        try:
+            b, e = slices(len(probe_key))[t]
+            sums[t] = hj.probe_sum(probe_key[b:e], probe_pay[b:e])
+        except Exception as ex:
+            errors.append(ex)
+
+    run(build)
+    run(probe)
+    return sum(sums) & 0xFFFFFFFFFFFFFFFF
+
+
 # ---------------------------------------------------------------------------
 # gpu_radix_join execution method
 # ---------------------------------------------------------------------------

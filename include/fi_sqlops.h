@@ -417,6 +417,44 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
                                       uint64_t len, uint64_t *result_set,
                                       uint64_t result_len, fi_stream_t stream);
 
+/* ---- CpuHashJoin: no-partitioning join on the host
+ *      (sql-ops/src/join/no_partitioning_join.rs:281-304, impl :440-560;
+ *      kernels sql-ops/cpputils/no_partitioning_join.cpp:27-273) -------- */
+typedef struct fi_cpu_hash_join fi_cpu_hash_join;
+
+/* HashTable::new_on_cpu (no_partitioning_join.rs:568-581): sets every key of
+ * `entries` host entries of {key, value} to the null key. */
+int fi_cpu_hash_table_init_int32(void *table, uint64_t entries);
+int fi_cpu_hash_table_init_int64(void *table, uint64_t entries);
+
+/* CpuHashJoinBuilder::build (no_partitioning_join.rs:765-772).  The table
+ * holds mem_len host entries; size (1..mem_len) is the size used for
+ * hashing.  The handle does not own the table.  Schemes: PERFECT,
+ * LINEAR_PROBING. */
+int fi_cpu_hash_join_new(fi_hashing_scheme hashing_scheme, int is_selective,
+                         void *hash_table, uint64_t mem_len, uint64_t size,
+                         fi_cpu_hash_join **out);
+void fi_cpu_hash_join_free(fi_cpu_hash_join *hj);
+
+/* CpuHashJoin::build (no_partitioning_join.rs:286-288, impl :446-505).
+ * Several threads may build disjoint slices into one table at once.
+ * InvalidArgument when len exceeds mem_len; Unsupported for a selective
+ * linear-probing build (unimplemented in the reference). */
+int fi_cpu_hash_join_build_int32(fi_cpu_hash_join *hj, const int32_t *key,
+                                 const int32_t *pay, uint64_t len);
+int fi_cpu_hash_join_build_int64(fi_cpu_hash_join *hj, const int64_t *key,
+                                 const int64_t *pay, uint64_t len);
+
+/* CpuHashJoin::probe_sum (no_partitioning_join.rs:296-303, impl :507-553):
+ * adds (wrapping) the payloads of all matches to *join_result; threads may
+ * probe disjoint slices into one result. */
+int fi_cpu_hash_join_probe_sum_int32(fi_cpu_hash_join *hj, const int32_t *key,
+                                     const int32_t *pay, uint64_t len,
+                                     uint64_t *join_result);
+int fi_cpu_hash_join_probe_sum_int64(fi_cpu_hash_join *hj, const int64_t *key,
+                                     const int64_t *pay, uint64_t len,
+                                     uint64_t *join_result);
+
 /* ---- gpu_radix_join execution method
  *      (radix-join/src/execution_methods/gpu_radix_join.rs:90-565) ------ */
 
