@@ -434,7 +434,7 @@ def run_ours(a):
         e2e = {"value": world * 2 * n / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * n * 8, "d2h_bytes_per_step": 16,
                "ms_per_step": e2e_ms,
-               "path": "fi_radix_join_engine_run_host_int64 (pinned host columns)"}
+               "path": "fi_radix_join_engine_run_host_int64 (pinned host columns; the first pass streamed block by block behind the copy)"}
         del host
 
     cpu = None

@@ -805,12 +805,27 @@ extern "C" int fi_radix_join_engine_run_int64(
 }
 
 template <typename K>
+static int engine_run_streamed(fi_radix_join_engine *e, const K *bk,
+                               const K *bp, uint64_t bn, const K *pk,
+                               const K *pp, uint64_t pn, uint64_t block_tuples,
+                               fi_join_result *result, cudaStream_t st);
+uint64_t host_stream_block(uint64_t maxn, uint32_t c1);
+
+// Host columns.  With two passes the columns are streamed block by block
+// (engine_run_streamed), so the copy of one block overlaps the first pass of
+// the one before and the host link is the only bound; one pass copies the
+// columns whole and runs the in-memory join.  Same results either way.
+template <typename K>
 static int engine_run_host(fi_radix_join_engine *e, const K *build_key,
                            const K *build_pay, uint64_t build_len,
                            const K *probe_key, const K *probe_pay,
                            uint64_t probe_len, fi_join_result *result,
                            cudaStream_t st) {
   if (!e || !result) return set_error(FI_ERR_INVALID_ARGUMENT, "null argument");
+  if (e->bits2 >= 0)
+    return engine_run_streamed<K>(
+        e, build_key, build_pay, build_len, probe_key, probe_pay, probe_len,
+        host_stream_block(std::max(build_len, probe_len), e->C1), result, st);
   const K *src[4] = {build_key, build_pay, probe_key, probe_pay};
   const uint64_t lens[4] = {build_len, build_len, probe_len, probe_len};
   for (int i = 0; i < 4; ++i) {
@@ -930,6 +945,14 @@ extern "C" int fi_radix_join_engine_set_plan(fi_radix_join_engine *e,
 // reference has no streamed radix join.
 constexpr uint64_t kStreamBlockDefault = 1ull << 26;  // tuples per block
 constexpr uint64_t kStreamBlockAlign = 1ull << 16;
+
+// Block size for run_host: the default, or larger when a relation would
+// otherwise need more blocks than the engine has pass-1 chunks.
+uint64_t host_stream_block(uint64_t maxn, uint32_t c1) {
+  uint64_t b = (maxn + c1 - 1) / c1;
+  b = (b + kStreamBlockAlign - 1) / kStreamBlockAlign * kStreamBlockAlign;
+  return std::max(b, kStreamBlockDefault);
+}
 
 template <typename K>
 static int engine_stream_pass1(fi_radix_join_engine *e, int r, const K *key,

@@ -595,7 +595,10 @@ int fi_radix_join_engine_run_int64(fi_radix_join_engine *e,
 
 /* Same join from host memory (ideally pinned): copies the four columns to
  * the device inside the call, runs the join and copies the result back into
- * the host `result`.  Synchronous. */
+ * the host `result`.  Synchronous.  With two radix passes the columns are
+ * streamed as by fi_radix_join_engine_run_streamed_* (blocks of 2^26 tuples,
+ * or len / SM count when larger), so the first pass overlaps the copy; with
+ * one pass they are copied whole first. */
 int fi_radix_join_engine_run_host_int32(fi_radix_join_engine *e,
                                         const int32_t *build_key,
                                         const int32_t *build_pay,

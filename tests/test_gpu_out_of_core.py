@@ -80,3 +80,24 @@ def test_streamed_validation(fi):
     assert ex.value.kind == "InvalidArgument"
     empty = torch.empty(0, dtype=torch.int64).pin_memory()
     assert two.run_streamed(empty, empty, kb, kb) == (0, 0)
+
+
+@pytest.mark.parametrize("bits", [(9,), (5, 7)])
+def test_run_host_one_and_two_passes(fi, bits):
+    """The host entry point: one pass copies the columns whole, two passes
+    stream them (here over two blocks of 2^26 tuples, the second ragged);
+    the same closed-form result either way, and for empty relations."""
+    n_b, n_p = 1 << 20, (1 << 26) + 54321
+    rk = torch.empty(n_b, dtype=torch.int32, device="cuda")
+    sk = torch.empty(n_p, dtype=torch.int32, device="cuda")
+    fi.gen_primary_keys(rk, 7)
+    fi.gen_uniform_foreign_keys(sk, n_b, 8)
+    exp = (int(sk.to(torch.int64).sum().item()), n_p)
+    hr, hs = rk.cpu().pin_memory(), sk.cpu().pin_memory()
+    del rk, sk
+    e = fi.RadixJoinEngine(n_b, n_p, torch.int32, fi.RadixBits(*bits),
+                           fi.HashingScheme.BucketChaining)
+    assert e.run_host(hr, hr, hs, hs) == exp
+    e.status()
+    assert e.run_host(hr[:0], hr[:0], hs, hs) == (0, 0)
+    assert e.run_host(hr, hr, hs, hs) == exp
