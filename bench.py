@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
                     choices=["join", "partition", "ooc", "serve", "dataset", "nopart",
-                             "hybrid"],
+                             "hybrid", "exchange"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
                          "join server against back-to-back plain calls; dataset: "
@@ -82,6 +82,12 @@ def parse():
     ap.add_argument("--ht-dim", default="0,256",
                     help="nopart workload: grid,block of build and probe (grid 0 "
                          "= 8 CTAs per SM)")
+    ap.add_argument("--exchange-log2n", type=int, default=29,
+                    help="exchange workload: int64 tuples one sender partitions "
+                         "and sends")
+    ap.add_argument("--exchange-ranks", type=int, default=8,
+                    help="exchange workload: receivers (power of two), emulated "
+                         "by local receive columns on this GPU")
     ap.add_argument("--ooc-log2n", type=int, default=31,
                     help="out-of-core join: |R| = |S| = 2^ooc_log2n int64 tuples")
     ap.add_argument("--ooc-block", type=int, default=0,
@@ -1107,6 +1113,98 @@ def run_nopart(a):
         dist.destroy_process_group()
 
 
+def run_exchange(a):
+    """The fused radix exchange kernel (partition + send into the receivers'
+    columns) on one GPU: one sender's 2^exchange_log2n int64 tuples go to
+    --exchange-ranks receivers whose receive columns are local buffers (on
+    several GPUs they are peer pointers and all but 1/W of the stores cross
+    NVLink).  A step = the destination histogram + the fused scatter.
+    Algorithmic bytes: key read (histogram) + tuple read + tuple write = 40
+    B/tuple; the scatter kernel alone 32 B/tuple."""
+    import torch
+    import fi_sqlops as fi
+    import distributed as D
+    world, rank, local = dist_setup(a.gpus)
+    n = 1 << a.exchange_log2n
+    W = a.exchange_ranks
+    g = D.exchange_bits(W)
+    shift = 18  # above 9+9 local join bits
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    pays = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_uniform_foreign_keys(keys, 1 << 40, a.seed + rank)
+    pays.copy_(keys)
+    counts = fi.exchange_histogram(keys, shift, g)
+    cnt = counts.cpu().tolist()
+    cols = [(torch.empty(max(c, 1), dtype=torch.int64, device="cuda"),
+             torch.empty(max(c, 1), dtype=torch.int64, device="cuda")) for c in cnt]
+    dests = [(k.data_ptr(), p.data_ptr(), 0, c) for (k, p), c in zip(cols, cnt)]
+    cursors = torch.empty(W, dtype=torch.int64, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(evs=None):
+        if evs: evs[0].record(stream)
+        fi.exchange_histogram(keys, shift, g, counts)
+        if evs: evs[1].record(stream)
+        fi.exchange_scatter(keys, pays, shift, g, dests, cursors, status)
+        if evs: evs[2].record(stream)
+
+    for _ in range(max(a.warmup, 3)):
+        step()
+    K = a.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(K):
+            step(ev[k])
+        torch.cuda.synchronize()
+        barrier(world)
+    # every receiver holds its tuples: counts, and key sums per destination
+    d_of = (keys >> shift) & (W - 1)
+    exp_sum = torch.zeros(W, dtype=torch.int64, device="cuda").index_add_(0, d_of, keys)
+    verified = int(status.item()) == 0 and cursors.cpu().tolist() == cnt
+    for d, (k, p) in enumerate(cols):
+        c = cnt[d]
+        verified = verified and int(k[:c].sum().item()) == int(exp_sum[d].item()) \
+            and bool(torch.equal(k[:c], p[:c]))
+    hist_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    scat_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    ms = max_over_ranks(hist_ms + scat_ms, world)
+    peak, peak_kind = load_peaks()
+    step_bytes, scat_bytes = n * 40, n * 32
+    nvlink_gbs = 770.0
+    if rank == 0:
+        line = {"metric": "radix exchange G tuples/s", "value": world * n / (ms / 1e3) / 1e9,
+                "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(a.warmup, 3),
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded uniform keys in [1, 2^40], payload = key)",
+                "config": {"workload": "radix_exchange_%dM_int64_%d_receivers_local" % (
+                               n >> 20, W),
+                           "tuples": n, "receivers": W, "exchange_bits": [shift, shift + g],
+                           "l2_flush": "none: inputs (%.1f GB) larger than L2" % (n * 16 / 1e9)},
+                "phases": {"histogram": {"ms": hist_ms,
+                                         "gb_per_s": n * 8 / (hist_ms / 1e3) / 1e9},
+                           "scatter": {"ms": scat_ms,
+                                       "gb_per_s": scat_bytes / (scat_ms / 1e3) / 1e9}},
+                "roofline": {"bound": "hbm", "kernel": "exchange_scatter",
+                             "achieved": scat_bytes / (scat_ms / 1e3) / 1e9, "peak": peak,
+                             "unit": "GB/s",
+                             "frac": scat_bytes / (scat_ms / 1e3) / 1e9 / peak,
+                             "peak_source": peak_kind, "traffic": None},
+                "pipeline_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                                      "achieved_gb_per_s": step_bytes / (ms / 1e3) / 1e9,
+                                      "frac_of_peak": step_bytes / (ms / 1e3) / 1e9 / peak},
+                "nvlink_bound_ms_on_%d_gpus" % W: n * 16 * (W - 1) / W / (nvlink_gbs * 1e9) * 1e3,
+                "gpu_launches": 2 * K,
+                "clocks": clk.summary(), "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def run_hybrid(a):
     """Hybrid join (the reference's cpu_partitioned_radix_join): host
     columns, first pass on all host threads, second pass and join on the GPU.
@@ -1181,6 +1279,8 @@ def main():
         run_nopart(a)
     elif a.workload == "hybrid":
         run_hybrid(a)
+    elif a.workload == "exchange":
+        run_exchange(a)
     else:
         run_ours(a)
 

@@ -12,10 +12,15 @@ the result equals the single-GPU join of the whole relations.
     dist.init_process_group("nccl", ...)        # one process per GPU
     s, c = exchange_join(rk, rp, sk, sp, bits=(9, 9))
 
-The grouping by destination is the library's radix partitioner (a
-Contiguous pass on the exchange bits); the all-to-all is NCCL's.  The
-exchange moves each tuple once over NVLink; a fused partition + peer-store
-kernel is the next step (it needs several GPUs to test).
+Two exchanges move each tuple once over NVLink:
+ * exchange="nccl": the library's radix partitioner groups the tuples by
+   destination (a Contiguous pass on the exchange bits), then NCCL's
+   all-to-all sends them;
+ * exchange="peer" (PeerExchange): one fused kernel partitions and stores
+   every tuple straight into the destination rank's receive columns, which
+   every rank maps by CUDA IPC.  The ranks' counts are all-gathered first,
+   so each sender owns a fixed region of every receiver's columns; no
+   kernel waits on another rank (the host orders the steps).
 """
 import torch
 import torch.distributed as dist
@@ -78,6 +83,119 @@ def shuffle(keys, pays, shift, group=None, group_by=gpu_group_by_destination):
     return out[:, 0].contiguous(), out[:, 1].contiguous()
 
 
+def region_bases(counts, rank):
+    """counts[s][d] = tuples sender s sends to rank d (a W x W list or
+    tensor).  Returns (base, recv): base[d] = first slot of `rank`'s region
+    in d's receive columns (the tuples of senders s < rank come first) and
+    recv[d] = tuples d receives in all."""
+    rows = [[int(x) for x in row] for row in (counts.tolist() if hasattr(counts, "tolist")
+                                               else counts)]
+    w = len(rows)
+    base = [sum(rows[s][d] for s in range(rank)) for d in range(w)]
+    recv = [sum(rows[s][d] for s in range(w)) for d in range(w)]
+    return base, recv
+
+
+def all_gather_counts(counts, group=None):
+    """The W x W count matrix (row s = sender s's counts) on every rank;
+    device tensors under NCCL, host tensors otherwise."""
+    world = dist.get_world_size(group)
+    if dist.get_backend(group) != "nccl":
+        counts = counts.cpu()
+    out = counts.new_empty(world * counts.numel())
+    dist.all_gather_into_tensor(out, counts.contiguous(), group=group)
+    return out.view(world, counts.numel()).cpu()
+
+
+_opened = {}  # IPC handle -> [mapped base pointer, users]: one mapping per allocation
+
+
+def _ipc_open(handle):
+    import fi_sqlops as fi
+    ent = _opened.get(handle)
+    if ent is None:
+        ent = _opened[handle] = [fi.ipc_open(handle), 0]
+    ent[1] += 1
+    return ent[0]
+
+
+def _ipc_release(handle):
+    import fi_sqlops as fi
+    ent = _opened[handle]
+    ent[1] -= 1
+    if ent[1] == 0:
+        del _opened[handle]
+        fi.ipc_close(ent[0])
+
+
+class PeerExchange:
+    """Receive columns of `capacity` tuples on every rank (keys, then
+    payloads, in one allocation), mapped into every other rank by CUDA IPC.
+    shuffle() sends each tuple to the rank given by its key bits
+    [shift, shift + g) with one fused partition + peer-store kernel and
+    returns the (keys, payloads) this rank received.
+
+    Order of a shuffle: histogram -> all-gather of the counts (a rendezvous:
+    no rank sends before every rank has finished with its columns) ->
+    capacity check on the shared matrix (every rank raises alike) -> fused
+    scatter -> synchronize -> barrier (every sender is done) -> read."""
+
+    def __init__(self, capacity, dtype, group=None, device=None):
+        import fi_sqlops as fi
+        self.group = group
+        self.world = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
+        self.g = exchange_bits(self.world)
+        self.capacity = capacity
+        dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.buf = torch.empty((2, max(capacity, 1)), dtype=dtype, device=dev)
+        self.keys, self.pays = self.buf[0], self.buf[1]
+        self.cursors = torch.empty(1 << self.g, dtype=torch.int64, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        handle, off = fi.ipc_handle(self.buf)
+        peers = [None] * self.world
+        dist.all_gather_object(peers, (handle, off, capacity), group=group)
+        self.handles, self.dests = [], []
+        for r, (h, o, cap) in enumerate(peers):
+            if r == self.rank:
+                self.dests.append((self.keys.data_ptr(), self.pays.data_ptr(), cap))
+            else:
+                base = _ipc_open(h)
+                self.handles.append(h)
+                pstep = max(cap, 1) * self.buf.element_size()
+                self.dests.append((base + o, base + o + pstep, cap))
+
+    def shuffle(self, keys, pays, shift):
+        import fi_sqlops as fi
+        counts = fi.exchange_histogram(keys, shift, self.g)
+        mat = all_gather_counts(counts, self.group)
+        base, recv = region_bases(mat, self.rank)
+        caps = [d[2] for d in self.dests]
+        if any(n > c for n, c in zip(recv, caps)):
+            raise fi.SqlOpsError(-7, "a rank receives %d tuples; its exchange holds %d"
+                                 % max(zip(recv, caps), key=lambda x: x[0] - x[1]))
+        dests = [(k, p, b, c) for (k, p, c), b in zip(self.dests, base)]
+        fi.exchange_scatter(keys, pays, shift, self.g, dests, self.cursors,
+                            self.status)
+        torch.cuda.synchronize()
+        dist.barrier(group=self.group)
+        code = int(self.status.item())
+        if code != 0:
+            self.status.zero_()
+            raise fi.SqlOpsError(code, "exchange scatter recorded an error")
+        n = recv[self.rank]
+        return self.keys[:n], self.pays[:n]
+
+    def close(self):
+        """Unmaps the peers' columns once every rank is done with them."""
+        if self.handles:
+            torch.cuda.synchronize()
+            dist.barrier(group=self.group)
+            for h in self.handles:
+                _ipc_release(h)
+            self.handles = []
+
+
 def gpu_local_join(rk, rp, sk, sp, bits, scheme):
     import fi_sqlops as fi
     e = fi.RadixJoinEngine(max(rk.numel(), 1), max(sk.numel(), 1), rk.dtype,
@@ -88,17 +206,43 @@ def gpu_local_join(rk, rp, sk, sp, bits, scheme):
 
 
 def exchange_join(rk, rp, sk, sp, bits=(9, 9), scheme=None, group=None,
-                  group_by=gpu_group_by_destination, local_join=gpu_local_join):
+                  group_by=gpu_group_by_destination, local_join=gpu_local_join,
+                  exchange="nccl", peers=None):
     """Join of R and S sharded over the ranks: exchange on the bits above
     the local join's, join locally, add up.  Returns (sum, count) of the
-    whole join on every rank."""
+    whole join on every rank.  exchange="peer" uses the fused kernel through
+    `peers` = (PeerExchange for R, PeerExchange for S), created here (and
+    closed again) when not given."""
     if scheme is None:
         import fi_sqlops as fi
         scheme = fi.HashingScheme.BucketChaining
     shift = sum(bits)
-    rk2, rp2 = shuffle(rk, rp, shift, group, group_by)
-    sk2, sp2 = shuffle(sk, sp, shift, group, group_by)
-    s, c = local_join(rk2, rp2, sk2, sp2, bits, scheme)
-    t = torch.tensor([s, c], dtype=torch.int64, device=rk.device)
+    if exchange == "peer":
+        own = peers is None
+        if own:  # receive columns sized to the largest share of each relation
+            import fi_sqlops as fi
+            g = exchange_bits(dist.get_world_size(group))
+            rank = dist.get_rank(group)
+            caps = [max(region_bases(all_gather_counts(
+                fi.exchange_histogram(k, shift, g), group), rank)[1])
+                for k in (rk, sk)]
+            peers = (PeerExchange(caps[0], rk.dtype, group),
+                     PeerExchange(caps[1], sk.dtype, group))
+        try:
+            rk2, rp2 = peers[0].shuffle(rk, rp, shift)
+            sk2, sp2 = peers[1].shuffle(sk, sp, shift)
+            s, c = local_join(rk2, rp2, sk2, sp2, bits, scheme)
+        finally:
+            if own:
+                for p in peers:
+                    p.close()
+    elif exchange == "nccl":
+        rk2, rp2 = shuffle(rk, rp, shift, group, group_by)
+        sk2, sp2 = shuffle(sk, sp, shift, group, group_by)
+        s, c = local_join(rk2, rp2, sk2, sp2, bits, scheme)
+    else:
+        raise ValueError("exchange must be 'nccl' or 'peer', got %r" % (exchange,))
+    dev = rk.device if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([s, c], dtype=torch.int64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return int(t[0].item()), int(t[1].item())

@@ -678,6 +678,74 @@ def cpu_hash_join_sum(build_key, build_pay, probe_key, probe_pay, hashing_scheme
 
 
 # ---------------------------------------------------------------------------
+# Radix exchange between GPUs (exchange.cu)
+# ---------------------------------------------------------------------------
+EXCHANGE_MAX_RANKS = 64
+IPC_HANDLE_BYTES = 64
+
+
+class ExchangeDest(C.Structure):
+    """fi_exchange_dest: one destination's receive columns (device or peer
+    pointers), the sender's first slot there and the columns' length."""
+    _fields_ = [("key", C.c_void_p), ("pay", C.c_void_p), ("base", C.c_uint64),
+                ("cap", C.c_uint64)]
+
+
+def exchange_histogram(keys, shift, exchange_bits, counts=None, stream=None):
+    """counts[d] = number of keys whose bits [shift, shift + exchange_bits)
+    equal d (an int64 device tensor of 2^exchange_bits entries)."""
+    F = 1 << exchange_bits
+    if counts is None:
+        counts = torch.empty(F, dtype=torch.int64, device=keys.device)
+    f = getattr(lib(), "fi_exchange_histogram_" + _sfx(keys.dtype))
+    _check(f(_ptr(keys), C.c_uint64(keys.numel()), C.c_uint32(shift),
+             C.c_uint32(exchange_bits), _ptr(counts), _stream(stream)))
+    return counts
+
+
+def exchange_scatter(keys, pays, shift, exchange_bits, dests, cursors=None,
+                     status=None, stream=None):
+    """Fused partition + send: dests is a list of 2^exchange_bits tuples
+    (key_ptr, pay_ptr, base, cap) -- device or peer pointers as ints.
+    Returns the cursors workspace (per destination: tuples sent)."""
+    F = 1 << exchange_bits
+    if len(dests) != F:
+        raise SqlOpsError(-1, "need %d destinations, got %d" % (F, len(dests)))
+    arr = (ExchangeDest * F)(*[ExchangeDest(int(k), int(p), int(b), int(c))
+                               for k, p, b, c in dests])
+    if cursors is None:
+        cursors = torch.empty(F, dtype=torch.int64, device=keys.device)
+    f = getattr(lib(), "fi_exchange_scatter_" + _sfx(keys.dtype))
+    _check(f(_ptr(keys), _ptr(pays), C.c_uint64(keys.numel()), C.c_uint32(shift),
+             C.c_uint32(exchange_bits), arr, _ptr(cursors), _ptr(status),
+             _stream(stream)))
+    return cursors
+
+
+def ipc_handle(t):
+    """(handle bytes, byte offset of t in its allocation): the CUDA IPC
+    handle of the whole allocation holding tensor t."""
+    buf = C.create_string_buffer(IPC_HANDLE_BYTES)
+    off = C.c_uint64(0)
+    _check(lib().fi_ipc_get_handle(_ptr(t), buf, C.byref(off)))
+    return buf.raw, off.value
+
+
+def ipc_open(handle):
+    """Opens another process's IPC handle; returns the allocation's base
+    device pointer (open each allocation once per process)."""
+    out = C.c_void_p()
+    _check(lib().fi_ipc_open_handle(C.create_string_buffer(bytes(handle),
+                                                           IPC_HANDLE_BYTES),
+                                    C.byref(out)))
+    return out.value
+
+
+def ipc_close(ptr):
+    _check(lib().fi_ipc_close_handle(C.c_void_p(ptr)))
+
+
+# ---------------------------------------------------------------------------
 # gpu_radix_join execution method
 # ---------------------------------------------------------------------------
 class RadixJoinEngine:

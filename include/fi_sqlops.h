@@ -455,6 +455,63 @@ int fi_cpu_hash_join_probe_sum_int64(fi_cpu_hash_join *hj, const int64_t *key,
                                      const int64_t *pay, uint64_t len,
                                      uint64_t *join_result);
 
+/* ---- Radix exchange between GPUs (no reference counterpart: the exchange
+ *      step of a distributed radix join; exchange.cu) --------------------- */
+#define FI_EXCHANGE_MAX_RANKS 64
+#define FI_IPC_HANDLE_BYTES 64
+
+/* One destination rank's receive columns as seen from the sending rank: a
+ * local device pointer for its own share, a peer pointer (opened with
+ * fi_ipc_open_handle) for the others.  The sender writes its tuples for
+ * this rank into slots [base, base + count) of both columns; cap is the
+ * columns' length, checked by every store. */
+typedef struct {
+  void *key;
+  void *pay;
+  uint64_t base;
+  uint64_t cap;
+} fi_exchange_dest;
+
+/* counts[d] (device u64[2^exchange_bits]) = number of keys whose bits
+ * [shift, shift + exchange_bits) equal d (key_to_partition of
+ * sql-ops/include/gpu_radix_partition.h:122-127 with ignore_bits = shift).
+ * exchange_bits <= 6; shift + exchange_bits <= the key's bit width. */
+int fi_exchange_histogram_int32(const int32_t *keys, uint64_t len, uint32_t shift,
+                                uint32_t exchange_bits, uint64_t *counts,
+                                fi_stream_t stream);
+int fi_exchange_histogram_int64(const int64_t *keys, uint64_t len, uint32_t shift,
+                                uint32_t exchange_bits, uint64_t *counts,
+                                fi_stream_t stream);
+
+/* Partition + send in one kernel: every tuple goes to destination d =
+ * its key bits [shift, shift + exchange_bits) and is stored into
+ * dests[d] (host array of 2^exchange_bits entries) at a slot in
+ * [base, base + counts[d]); the order within the region is unspecified.
+ * cursors: device u64[2^exchange_bits] workspace.  A store beyond cap is
+ * skipped and FI_ERR_CAPACITY recorded in the device word *status (may be
+ * null).  No kernel waits on another rank; the caller orders the ranks'
+ * steps (synchronize, then a process-group barrier, before the receivers
+ * read). */
+int fi_exchange_scatter_int32(const int32_t *keys, const int32_t *pays, uint64_t len,
+                              uint32_t shift, uint32_t exchange_bits,
+                              const fi_exchange_dest *dests, uint64_t *cursors,
+                              int *status, fi_stream_t stream);
+int fi_exchange_scatter_int64(const int64_t *keys, const int64_t *pays, uint64_t len,
+                              uint32_t shift, uint32_t exchange_bits,
+                              const fi_exchange_dest *dests, uint64_t *cursors,
+                              int *status, fi_stream_t stream);
+
+/* CUDA IPC for the receive columns.  fi_ipc_get_handle: the handle
+ * (FI_IPC_HANDLE_BYTES) of the whole allocation holding dev_ptr (e.g. a
+ * block of a caching allocator) and dev_ptr's offset in it.
+ * fi_ipc_open_handle (another process, another GPU): the allocation's base
+ * as a peer pointer (peer access enabled lazily); add the offset.  An
+ * allocation is opened once per process: callers share one mapping among
+ * equal handles.  fi_ipc_close_handle takes the opened base. */
+int fi_ipc_get_handle(const void *dev_ptr, void *handle, uint64_t *offset);
+int fi_ipc_open_handle(const void *handle, void **base);
+int fi_ipc_close_handle(void *base);
+
 /* ---- gpu_radix_join execution method
  *      (radix-join/src/execution_methods/gpu_radix_join.rs:90-565) ------ */
 

@@ -95,3 +95,47 @@ def test_exchange_needs_power_of_two():
     with pytest.raises(ValueError):
         D.exchange_bits(3)
     assert D.exchange_bits(8) == 3
+
+
+def plan_worker(rank, world, port, out):
+    """The peer exchange's plan on gloo ranks: all-gathered counts and each
+    sender's region in every receiver's columns."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        import distributed as D
+        g = D.exchange_bits(world)
+        keys = torch.from_numpy(np.random.default_rng(rank).integers(
+            0, 1 << 20, 1000 + 337 * rank))
+        counts = torch.bincount(D.destinations(keys, 12, g), minlength=world)
+        mat = D.all_gather_counts(counts)
+        base, recv = D.region_bases(mat, rank)
+        out.put((rank, mat.tolist(), base, recv, counts.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_peer_exchange_plan(world):
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    mp.spawn(plan_worker, args=(world, free_port(), out), nprocs=world, join=True)
+    got = sorted(out.get(timeout=60) for _ in range(world))
+    mats = [g[1] for g in got]
+    assert all(m == mats[0] for m in mats)  # every rank sees one matrix
+    for rank, mat, base, recv, counts in got:
+        assert mat[rank] == counts  # row s = sender s's counts
+        assert recv == [sum(mat[s][d] for s in range(world)) for d in range(world)]
+    for d in range(world):  # the senders' regions tile each receiver's columns
+        spans = sorted((got[s][2][d], got[s][2][d] + mats[0][s][d]) for s in range(world))
+        assert spans[0][0] == 0 and spans[-1][1] == got[0][3][d]
+        assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+
+
+def test_region_bases_small():
+    import distributed as D
+    mat = [[3, 1], [2, 5]]
+    assert D.region_bases(mat, 0) == ([0, 0], [5, 6])
+    assert D.region_bases(mat, 1) == ([3, 1], [5, 6])
