@@ -28,7 +28,8 @@
 //  * Probe tuples stream in with 16-byte evict-first loads, several per
 //    thread in flight.  When an item starts, its CTA issues one
 //    prefetch.global.L2 per 128-byte line of the item's build range (unless
-//    the table is kept) and probe range, so the build and probe iterations
+//    the table is kept) and of the first kProbePrefetch tuples of its probe
+//    range, so the build and probe iterations
 //    after the first find their lines in L2 instead of paying a DRAM round
 //    trip each: 7.49 -> 6.61 ms for the 1024M x 1024M int64 join.  Also
 //    prefetching the next item's build lines when this item's probe starts
@@ -56,6 +57,14 @@ namespace fi {
 
 constexpr uint32_t kPlanThreads = 1024;
 constexpr uint32_t kProbeUnroll = 4;
+// Probe tuples of an item prefetched into L2 when it starts.  Prefetching
+// all of a long item (a Zipf-hot partition's items hold 450K tuples, the
+// Blanas data set's 64K) fills L2 with lines evicted before their use: the
+// join at Zipf 1.5 took 9.19 ms with it, 7.94 ms with this cap (uniform:
+// 6.61 and 6.63 ms).  A rolling window of 4096 tuples kept ahead of the
+// probe loop gave 7.84 ms, but its extra code in the loop cost the uniform
+// join 0.13 ms.
+constexpr uint32_t kProbePrefetch = 8192;
 
 // ---- reference greedy task assignment --------------------------------------
 // Same result as gpu_radix_join_assign_tasks (radix_join.cu:58-98), with the
@@ -380,7 +389,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) radix_join_kernel(
       constexpr uint32_t kLine = 128 / sizeof(Tuple<K>);
       const uint32_t bn = (cached_p == (int64_t)p && bsize <= cap)
                               ? 0u : (uint32_t)min(bsize, (uint64_t)cap);
-      const uint32_t qn = (uint32_t)(qe - qb);
+      const uint32_t qn = (uint32_t)min(qe - qb, (uint64_t)kProbePrefetch);
       for (uint32_t i = tid * kLine; i < bn; i += nt * kLine) prefetch_l2(build + bb + i);
       for (uint32_t i = tid * kLine; i < qn; i += nt * kLine) prefetch_l2(probe + qb + i);
     }
