@@ -1085,6 +1085,9 @@ def run_nopart(a):
     # write an entry), probe (read a tuple, read an entry)
     build_bytes = size * tb + nb * 2 * tb
     probe_bytes = npr * 2 * tb
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        cpu = nopart_cpu_baseline(rk, rp, sk, sp, size, perfect)
     if rank == 0:
         line = {"metric": "no-partitioning join G tuples/s", "value": value,
                 "unit": UNIT, "n_gpus": world, "steps": K, "warmup": a.warmup,
@@ -1106,11 +1109,40 @@ def run_nopart(a):
                              "peak": peak, "unit": "GB/s",
                              "frac": probe_bytes / (probe_ms / 1e3) / 1e9 / peak,
                              "peak_source": peak_kind, "traffic": None},
+                "cpu_baseline": cpu,
                 "clocks": clk.summary(), "verified": bool(verified)}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def nopart_cpu_baseline(rk, rp, sk, sp, size, perfect):
+    """The reference's own CPU no-partitioning join (cpu_ht_build_* +
+    cpu_ht_probe_aggregate_*, compiled from its sources; single-threaded
+    as the reference's kernels are) on the whole build side and the first
+    eighth of the probe side, with the same table size."""
+    import oracle as O
+    npr = max(1, sk.numel() // 8)
+    r, p = rk.cpu().numpy(), rp.cpu().numpy()
+    s, q = sk[:npr].cpu().numpy(), sp[:npr].cpu().numpy()
+    kind = "reference" if O.ref_available() else "port"
+    if perfect:  # the perfect kernels index the table with the key unchecked:
+        # null build keys need the selective build, probe keys lie in 1..|R|
+        sel = bool((r == -1).any())
+        f = O.ref_ht_perfect_sum if kind == "reference" else O.ht_perfect_sum
+        fn = lambda *x: f(*x, selective=sel)
+    else:
+        fn = O.ref_ht_linearprobing_sum if kind == "reference" else O.ht_linearprobing_sum
+    t0 = time.perf_counter()
+    fn(r, p, s, q, size)
+    sec = time.perf_counter() - t0
+    return {"value": (len(r) + npr) / sec / 1e9, "unit": UNIT, "cores": 1,
+            "kind": kind,
+            "sample": "build all %d tuples, probe the first %d (1/8) of the same "
+                      "data, %d-entry %s table; one run" % (
+                          len(r), npr, size, "perfect" if perfect else "linear-probing"),
+            "seconds": sec}
 
 
 def run_exchange(a):
