@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <emmintrin.h>
 #include <new>
 #include <vector>
 
@@ -67,6 +68,7 @@ struct fi_cpu_radix_partitioner {
   uint32_t radix_bits;
   std::vector<uint64_t> cursors;   // F
   std::vector<uint32_t> fill;      // SWWC: tuples buffered per partition
+  std::vector<uint32_t> lo;        // SWWC: first slot of a line that is ours
   unsigned char *lines = nullptr;  // SWWC: F line buffers, 64-byte aligned
   ~fi_cpu_radix_partitioner() { ::operator delete[](lines, std::align_val_t(fi::kLineBytes)); }
 };
@@ -92,6 +94,7 @@ extern "C" int fi_cpu_radix_partitioner_new(fi_cpu_histogram_algorithm histogram
   p->radix_bits = radix_bits;
   const uint32_t F = 1u << radix_bits;
   p->cursors.resize(F);
+  p->lo.resize(F);
   if (algorithm != FI_CPU_PARTITION_NC) {
     p->fill.resize(F);
     p->lines = static_cast<unsigned char *>(
@@ -134,6 +137,62 @@ int cpu_prefix_sum(fi_cpu_radix_partitioner *p, const K *keys, uint64_t data_len
   return FI_OK;
 }
 
+// SWWC with line-aligned flushes (relation base aligned to the tuple size).
+// Each partition's buffer mirrors the 64-byte line of the relation that its
+// next tuple lands in: the first line of a partition starts at the slot
+// its first tuple takes (the slots before it belong to the previous
+// partition or its padding and are not written), every later line is
+// whole and aligned and goes out with non-temporal 16-byte stores (no
+// read-for-ownership of the destination), the last one with plain stores.
+// p->cursors holds the partition offsets on entry.
+template <typename K>
+int swwc_aligned(fi_cpu_radix_partitioner *p, const K *keys, const K *pays,
+                 const ChunkRange &r, uint32_t F, uint64_t mask, uint32_t ignore_bits,
+                 Tuple<K> *out, uint64_t out_len) {
+  constexpr uint32_t T = sizeof(Tuple<K>), B = kLineBytes / T;
+  Tuple<K> *lines = reinterpret_cast<Tuple<K> *>(p->lines);
+  uint32_t *fill = p->fill.data(), *lo = p->lo.data();
+  uint64_t *lb = p->cursors.data();  // index of the line's slot 0 (mod 2^64)
+  const uintptr_t base = reinterpret_cast<uintptr_t>(out);
+  for (uint32_t q = 0; q < F; ++q) {
+    const uint32_t off = (uint32_t)(((base + lb[q] * T) % kLineBytes) / T);
+    fill[q] = lo[q] = off;
+    lb[q] -= off;
+  }
+  for (uint64_t i = r.begin; i < r.end; ++i) {
+    const K k = keys[i];
+    const uint32_t q = cpu_partition_of(k, mask, ignore_bits);
+    Tuple<K> *line = lines + (size_t)q * B;
+    line[fill[q]] = Tuple<K>{k, pays[i]};
+    if (++fill[q] == B) {
+      if (lb[q] + B > out_len)
+        return set_error(FI_ERR_CAPACITY, "partition offsets point outside the relation");
+      if (lo[q] == 0) {
+        const __m128i *src = reinterpret_cast<const __m128i *>(line);
+        __m128i *dst = reinterpret_cast<__m128i *>(out + lb[q]);
+        _mm_stream_si128(dst + 0, _mm_load_si128(src + 0));
+        _mm_stream_si128(dst + 1, _mm_load_si128(src + 1));
+        _mm_stream_si128(dst + 2, _mm_load_si128(src + 2));
+        _mm_stream_si128(dst + 3, _mm_load_si128(src + 3));
+      } else {
+        std::memcpy(out + (lb[q] + lo[q]), line + lo[q], (B - lo[q]) * T);
+        lo[q] = 0;
+      }
+      lb[q] += B;
+      fill[q] = 0;
+    }
+  }
+  for (uint32_t q = 0; q < F; ++q)
+    if (fill[q] > lo[q]) {
+      if (lb[q] + fill[q] > out_len)
+        return set_error(FI_ERR_CAPACITY, "partition offsets point outside the relation");
+      std::memcpy(out + (lb[q] + lo[q]), lines + (size_t)q * B + lo[q],
+                  (fill[q] - lo[q]) * T);
+    }
+  _mm_sfence();  // the streamed lines are visible before the caller reads them
+  return FI_OK;
+}
+
 template <typename K>
 int cpu_partition(fi_cpu_radix_partitioner *p, const K *keys, const K *pays,
                   uint64_t data_len, uint32_t chunk_id, uint32_t num_chunks,
@@ -163,6 +222,8 @@ int cpu_partition(fi_cpu_radix_partitioner *p, const K *keys, const K *pays,
   constexpr uint32_t B = kLineBytes / sizeof(Tuple<K>);
   Tuple<K> *lines = reinterpret_cast<Tuple<K> *>(p->lines);
   uint32_t *fill = p->fill.data();
+  if (reinterpret_cast<uintptr_t>(out) % sizeof(Tuple<K>) == 0)
+    return swwc_aligned<K>(p, keys, pays, r, F, mask, ignore_bits, out, out_len);
   std::memset(fill, 0, (size_t)F * sizeof(uint32_t));
   for (uint64_t i = r.begin; i < r.end; ++i) {
     const K k = keys[i];
