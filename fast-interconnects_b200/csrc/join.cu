@@ -47,7 +47,9 @@
 //    flight per thread instead of four: 9.16 ms (register spills), or 8.20
 //    ms with three 256-thread CTAs per SM to give them the registers: the
 //    number of partitions an SM works on at once matters more than the
-//    loads each thread keeps in flight.
+//    loads each thread keeps in flight.  u16 bucket heads (twice the
+//    buckets in the same shared memory, chains half as long) with a 16-bit
+//    CAS-loop exchange in the build: join 6.61 -> 8.06 ms.
 #include <atomic>
 
 #include "common.cuh"
