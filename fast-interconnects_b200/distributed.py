@@ -138,7 +138,8 @@ class PeerExchange:
     Order of a shuffle: histogram -> all-gather of the counts (a rendezvous:
     no rank sends before every rank has finished with its columns) ->
     capacity check on the shared matrix (every rank raises alike) -> fused
-    scatter -> synchronize -> barrier (every sender is done) -> read."""
+    scatter -> synchronize -> all-reduce of the senders' status (every
+    sender is done; an error on any rank raises on every rank) -> read."""
 
     def __init__(self, capacity, dtype, group=None, device=None):
         import fi_sqlops as fi
@@ -177,19 +178,26 @@ class PeerExchange:
         dests = [(k, p, b, c) for (k, p, c), b in zip(self.dests, base)]
         fi.exchange_scatter(keys, pays, shift, self.g, dests, self.cursors,
                             self.status)
-        torch.cuda.synchronize()
-        dist.barrier(group=self.group)
-        code = int(self.status.item())
+        if self.buf.is_cuda:
+            torch.cuda.synchronize()
+        # every sender is done; a status recorded by any sender fails every
+        # rank alike (a receiver's columns are incomplete then)
+        st = self.status.to(torch.int32).reshape(1).clone()
+        if dist.get_backend(self.group) != "nccl":
+            st = st.cpu()
+        dist.all_reduce(st, op=dist.ReduceOp.MIN, group=self.group)
+        code = int(st.item())
         if code != 0:
             self.status.zero_()
-            raise fi.SqlOpsError(code, "exchange scatter recorded an error")
+            raise fi.SqlOpsError(code, "exchange scatter recorded an error on a rank")
         n = recv[self.rank]
         return self.keys[:n], self.pays[:n]
 
     def close(self):
         """Unmaps the peers' columns once every rank is done with them."""
         if self.handles:
-            torch.cuda.synchronize()
+            if self.buf.is_cuda:
+                torch.cuda.synchronize()
             dist.barrier(group=self.group)
             for h in self.handles:
                 _ipc_release(h)

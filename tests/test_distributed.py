@@ -139,3 +139,91 @@ def test_region_bases_small():
     mat = [[3, 1], [2, 5]]
     assert D.region_bases(mat, 0) == ([0, 0], [5, 6])
     assert D.region_bases(mat, 1) == ([3, 1], [5, 6])
+
+
+def peer_protocol_worker(rank, world, port, out):
+    """PeerExchange's host protocol on gloo ranks, with the two kernels and
+    CUDA IPC replaced by host fakes: the fake scatter records what it was
+    given and writes this rank's own share into its own columns."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        import distributed as D
+        import fi_sqlops as fi
+        g = D.exchange_bits(world)
+        state = {"calls": [], "fail_rank": None, "ex": None}
+
+        def hist(keys, shift, gg, counts=None, stream=None):
+            return torch.bincount(D.destinations(keys, shift, gg), minlength=1 << gg)
+
+        def scatter(keys, pays, shift, gg, dests, cursors=None, status=None, stream=None):
+            state["calls"].append([(int(k), int(p), int(b), int(c)) for k, p, b, c in dests])
+            d = D.destinations(keys, shift, gg)
+            ex, sel = state["ex"], d == rank
+            b = int(dests[rank][2])
+            ex.keys[b:b + int(sel.sum())] = keys[sel]
+            ex.pays[b:b + int(sel.sum())] = pays[sel]
+            if state["fail_rank"] == rank:
+                status.fill_(-7)
+            return cursors
+
+        fi.exchange_histogram, fi.exchange_scatter = hist, scatter
+        fi.ipc_handle = lambda t: (b"h%d" % rank, 16 * rank)
+        fi.ipc_open = lambda h: 1 << (20 + int(h[1:]))
+        fi.ipc_close = lambda ptr: None
+        rng = np.random.default_rng(rank)
+        keys = torch.from_numpy(rng.integers(0, 1 << 16, 5000 + 1000 * rank))
+        cap = 8000
+        ex = D.PeerExchange(cap, torch.int64, device="cpu")
+        state["ex"] = ex
+        got_k, got_p = ex.shuffle(keys, keys * 3, 10)
+        b_self = state["calls"][0][rank][2]
+        n_self = int((D.destinations(keys, 10, g) == rank).sum())
+        own_k, own_p = got_k[b_self:b_self + n_self], got_p[b_self:b_self + n_self]
+        res = {"calls": state["calls"][0], "n": len(got_k),
+               "mine_ok": bool((D.destinations(own_k, 10, g) == rank).all())
+               and bool(torch.equal(own_p, own_k * 3))}
+        # a sender's recorded error fails both ranks alike
+        state["fail_rank"] = 1
+        try:
+            ex.shuffle(keys, keys, 10)
+            res["status_raised"] = False
+        except fi.SqlOpsError as e:
+            res["status_raised"] = e.code == -7
+        # too little room anywhere: every rank raises before sending
+        small = D.PeerExchange(100, torch.int64, device="cpu")
+        try:
+            small.shuffle(keys, keys, 10)
+            res["cap_raised"] = False
+        except fi.SqlOpsError as e:
+            res["cap_raised"] = e.code == -7
+        dist.barrier()  # the group still works after both errors
+        small.close()
+        ex.close()
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_peer_exchange_protocol_two_ranks():
+    import distributed as D
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    mp.spawn(peer_protocol_worker, args=(2, free_port(), out), nprocs=2, join=True)
+    got = dict(out.get(timeout=60) for _ in range(2))
+    # rebuild the count matrix the ranks shared
+    mats = []
+    for r in range(2):
+        keys = torch.from_numpy(np.random.default_rng(r).integers(0, 1 << 16, 5000 + 1000 * r))
+        mats.append(torch.bincount(D.destinations(keys, 10, 1), minlength=2).tolist())
+    for r in range(2):
+        res = got[r]
+        base, recv = D.region_bases(mats, r)
+        assert res["n"] == recv[r] and res["mine_ok"]
+        assert res["status_raised"] and res["cap_raised"]
+        for d, (kp, pp, b, c) in enumerate(res["calls"]):
+            assert (b, c) == (base[d], 8000)
+            if d != r:  # the peer's columns: mapped base + its offset, payloads after keys
+                assert kp == (1 << (20 + d)) + 16 * d and pp == kp + 8000 * 8
