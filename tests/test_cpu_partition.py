@@ -75,3 +75,31 @@ def test_cpu_partition_errors(fi, oracle):
     with pytest.raises(fi.SqlOpsError) as ex:
         p.partition(keys, keys, 0, 1, off, small)
     assert ex.value.kind == "Capacity"
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+def test_cpu_swwc_unaligned_relation(fi, oracle, dtype):
+    """A relation whose base is not aligned to the tuple size takes the
+    plain-copy write-combining path; its slots equal the oracle's too, as do
+    those of the line-aligned streaming path on an aligned relation."""
+    n, bits, chunks = 50_001, 6, 3
+    keys = oracle.uniform_u64_keys(n, 17).astype(dtype)
+    pays = oracle.uniform_u64_keys(n, 18).astype(dtype)
+    F, pad = 1 << bits, fi.padding_len(fi.torch.int32 if dtype == np.int32 else fi.torch.int64)
+    tsz = 2 * np.dtype(dtype).itemsize
+    total = n + chunks * F * pad
+    raw = np.zeros(total * tsz + 64, np.uint8)
+    base = raw.ctypes.data
+    skew = (tsz // 2 - base % tsz) % tsz or tsz // 2  # element-aligned, not tuple-aligned
+    rel = raw[skew:skew + total * tsz].view(dtype).reshape(total, 2)
+    assert rel.ctypes.data % tsz != 0 and rel.ctypes.data % np.dtype(dtype).itemsize == 0
+    rel[:] = -1
+    off = np.zeros(chunks * F, np.uint64)
+    p = fi.CpuRadixPartitioner(fi.CpuHistogramAlgorithm.Chunked,
+                               fi.CpuRadixPartitionAlgorithm.SWWC, bits)
+    for c in range(chunks):
+        o = off[c * F:(c + 1) * F]
+        p.prefix_sum(keys, c, chunks, o)
+        p.partition(keys, pays, c, chunks, o, rel)
+    exp = oracle.chunked_radix_partition(keys, pays, off, chunks, bits, 0, total)
+    assert np.array_equal(rel, exp)
