@@ -333,3 +333,64 @@ def test_engine_probe_before_build(fi):
     with pytest.raises(fi.SqlOpsError) as ex:
         e.probe(k, k)
     assert ex.value.kind == "InvalidArgument"
+
+
+# --------------------------------------------------------------------------
+# The join-pinning fixtures (tests/golden/make_golden.py): misses, duplicate
+# build keys, negative keys and payloads, mostly empty partitions.  The CUDA
+# joins are compared with the sums and counts of the reference's own compiled
+# join directly, not only with the oracle.
+# --------------------------------------------------------------------------
+import os  # noqa: E402
+
+_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_cpu_ops.npz")
+PIN_KINDS = ("misses", "duplicates", "negative", "sparse")
+PIN_PERFECT = ("misses", "sparse")
+
+
+def _pin_case(kind, name):
+    g = np.load(_GOLDEN)
+    pre = "join_pin_%s_%s_" % (kind, name)
+    return (g[pre + "r_key"], g[pre + "r_pay"], g[pre + "s_key"], g[pre + "s_pay"],
+            int(g[pre + "sum"][0]), int(g[pre + "count"][0]))
+
+
+@pytest.mark.parametrize("kind", PIN_KINDS)
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["Perfect", "BucketChaining"])
+@pytest.mark.parametrize("bits", [0, 4, 6])
+def test_radix_join_pinned_to_reference(fi, kind, ndt, tdt, scheme, bits):
+    if scheme == "Perfect" and kind not in PIN_PERFECT:
+        pytest.skip("perfect hashing needs unique non-negative build keys")
+    name = "i32" if ndt == np.int32 else "i64"
+    rk, rp, sk, sp, exp_s, exp_c = _pin_case(kind, name)
+    b = partition_contiguous(fi, to_dev(rk), to_dev(rp), bits)
+    pr = partition_contiguous(fi, to_dev(sk), to_dev(sp), bits)
+    grid, block = 37, 512
+    result = torch.zeros(grid * block, dtype=torch.int64, device="cuda")
+    tasks = torch.zeros(grid + 1, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    j = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(bits),
+                         getattr(fi.HashingScheme, scheme), grid, block)
+    j.join(b, pr, result, tasks, match_count=count)
+    j.status()
+    got = int(to_host(result).astype(np.int64).sum(dtype=np.int64)) & ((1 << 64) - 1)
+    assert (got, int(to_host(count)[0])) == (exp_s, exp_c)
+
+
+@pytest.mark.parametrize("kind", PIN_KINDS)
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("bits,scheme", [((5,), "BucketChaining"),
+                                         ((3, 3), "BucketChaining"),
+                                         ((3, 3), "Perfect"),
+                                         ((2, 4), "BucketChaining")])
+def test_engine_pinned_to_reference(fi, kind, ndt, tdt, bits, scheme):
+    if scheme == "Perfect" and kind not in PIN_PERFECT:
+        pytest.skip("perfect hashing needs unique non-negative build keys")
+    name = "i32" if ndt == np.int32 else "i64"
+    rk, rp, sk, sp, exp_s, exp_c = _pin_case(kind, name)
+    e = fi.RadixJoinEngine(len(rk), len(sk), tdt, fi.RadixBits(*bits),
+                           getattr(fi.HashingScheme, scheme))
+    s, c = e.run(to_dev(rk), to_dev(rp), to_dev(sk), to_dev(sp))
+    e.status()
+    assert (s & ((1 << 64) - 1), c) == (exp_s, exp_c)

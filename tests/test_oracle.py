@@ -122,3 +122,97 @@ def test_datagen_shapes(oracle):
     # P(rank 1) = 1 / H_{N,1.5} ~ 0.383
     assert 0.37 < cnt.max() / len(z) < 0.40
     assert set(np.unique(z)) <= set(oracle.primary_keys(100000, 9, np.int64))
+
+
+# --------------------------------------------------------------------------
+# The radix-join restatement pinned to the reference's own join code.
+# The reference's linear-probing join (no_partitioning_join.cpp:27-140) adds
+# s.value once per build tuple with an equal key, which is what the radix
+# join aggregates (radix_join.cu:103-311); the match count is the same join
+# with every probe payload set to 1.  Cases: about half of the probe tuples
+# missing, duplicate build keys, negative keys and payloads (int32 sign
+# extension through key_to_partition), and all but one partition empty.
+# --------------------------------------------------------------------------
+import importlib.util as _ilu  # noqa: E402
+
+_spec = _ilu.spec_from_file_location(
+    "make_golden", os.path.join(os.path.dirname(__file__), "golden", "make_golden.py"))
+make_golden = _ilu.module_from_spec(_spec)
+_spec.loader.exec_module(make_golden)
+
+PIN_DTYPES = [("i32", np.int32), ("i64", np.int64)]
+# the perfect scheme is defined for unique, non-negative build keys
+PERFECT_KINDS = ("misses", "sparse")
+
+
+def _one_pass_join(oracle, scheme, rk, rp, sk, sp, bits):
+    """Partition both sides into one contiguous relation (Chunked, one chunk)
+    and run the oracle's per-partition join on it."""
+    pad = oracle.padding_len(rk.dtype)
+    F = 1 << bits
+    rels = []
+    for k, v in ((rk, rp), (sk, sp)):
+        off = oracle.chunked_prefix_sum(k, 1, bits)
+        rels.append((oracle.chunked_radix_partition(k, v, off, 1, bits, 0,
+                                                    len(k) + F * pad), off))
+    (b_rel, b_off), (p_rel, p_off) = rels
+    entries = 1
+    if scheme == "perfect":
+        entries = int(max(int(rk.max()), int(sk.max()))) // F + 1
+    return oracle.radix_join(scheme, b_rel, b_off, pad, p_rel, p_off, pad, bits,
+                             bits, ht_entries=entries)
+
+
+@pytest.mark.parametrize("kind", make_golden.JOIN_PIN_KINDS)
+@pytest.mark.parametrize("name,dt", PIN_DTYPES)
+@pytest.mark.parametrize("scheme", ["chaining", "perfect"])
+@pytest.mark.parametrize("bits", [0, 4, 6])
+def test_oracle_radix_join_matches_golden(oracle, golden, kind, name, dt, scheme,
+                                          bits):
+    if scheme == "perfect" and kind not in PERFECT_KINDS:
+        pytest.skip("perfect hashing needs unique non-negative build keys")
+    pre = "join_pin_%s_%s_" % (kind, name)
+    rk, rp = golden[pre + "r_key"], golden[pre + "r_pay"]
+    sk, sp = golden[pre + "s_key"], golden[pre + "s_pay"]
+    s, c = _one_pass_join(oracle, scheme, rk, rp, sk, sp, bits)
+    assert np.uint64(s % (1 << 64)) == golden[pre + "sum"][0]
+    assert c == int(golden[pre + "count"][0])
+
+
+@pytest.mark.parametrize("kind", make_golden.JOIN_PIN_KINDS)
+@pytest.mark.parametrize("bits1,bits2,threads", [(3, 3, 1), (5, 4, 4), (0, 6, 3)])
+def test_oracle_two_pass_join_matches_golden(oracle, golden, kind, bits1, bits2,
+                                             threads):
+    """The two-pass CPU radix join (pass 1, pass 2 over each first-pass
+    partition, bucket-chaining join) that the engine tests compare with."""
+    pre = "join_pin_%s_i64_" % kind
+    rk, rp = golden[pre + "r_key"], golden[pre + "r_pay"]
+    sk, sp = golden[pre + "s_key"], golden[pre + "s_pay"]
+    s, c, _, _ = oracle.cpu_radix_join(rk, rp, sk, sp, bits1, bits2, threads,
+                                       use_reference=False)
+    assert np.uint64(s % (1 << 64)) == golden[pre + "sum"][0]
+    assert c == int(golden[pre + "count"][0])
+
+
+@pytest.mark.parametrize("kind", make_golden.JOIN_PIN_KINDS)
+@pytest.mark.parametrize("name,dt", PIN_DTYPES)
+def test_oracle_radix_join_matches_compiled_reference(oracle, kind, name, dt):
+    """Larger inputs than the fixtures, against the compiled reference."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU library not built")
+    seed = 100 * make_golden.JOIN_PIN_KINDS.index(kind) + (32 if name == "i32" else 64)
+    rng = np.random.default_rng(seed)
+    rk, rp, sk, sp = make_golden.join_pin_inputs(kind, dt, rng, 40000, 90001)
+    exp_s, exp_c = make_golden.ref_join_sum_count(rk, rp, sk, sp)
+    for scheme in ("chaining", "perfect"):
+        if scheme == "perfect" and kind not in PERFECT_KINDS:
+            continue
+        for bits in (2, 7):
+            s, c = _one_pass_join(oracle, scheme, rk, rp, sk, sp, bits)
+            assert (np.uint64(s % (1 << 64)), c) == (np.uint64(exp_s), exp_c), (
+                scheme, bits)
+    if dt == np.int64:
+        for use_ref in (False, True):
+            s, c, _, _ = oracle.cpu_radix_join(rk, rp, sk, sp, 4, 5, 4,
+                                               use_reference=use_ref)
+            assert (np.uint64(s % (1 << 64)), c) == (np.uint64(exp_s), exp_c), use_ref
