@@ -18,10 +18,12 @@
 // the stream), so the contents left by a previous call do not matter.
 //
 // Host code cannot use the array's symbol as a device address: the symbol
-// is a host-side stand-in.  The device address is looked up once per device
-// with cudaGetSymbolAddress, with that device current, by the first call on
-// that device; make that first call before capturing the stream into a CUDA
-// graph.
+// is a host-side stand-in.  The device address is looked up with
+// cudaGetSymbolAddress, with that device current, by the first call on that
+// device; make that first call before capturing the stream into a CUDA
+// graph.  Calls made while the stream is not being captured look the address
+// up again, so a cudaDeviceReset (which unloads the module and may place the
+// array elsewhere when it is loaded again) between calls is harmless.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -42,15 +44,21 @@ static __device__ __align__(256) uint32_t g_noalloc_counters[kNoAllocCounters];
 std::mutex g_noalloc_mutex;
 uint32_t *g_noalloc_addr[kMaxDevices] = {};
 
-// Device address of g_noalloc_counters on the current device.
-int noalloc_scratch(uint32_t **out) {
+// Device address of g_noalloc_counters on the current device.  Looked up on
+// the first call on the device, and again on every call whose stream is not
+// being captured (a capture keeps the address recorded before it).
+int noalloc_scratch(cudaStream_t stream, uint32_t **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fi::cuda_error(e, "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices)
     return fi::set_error(FI_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const bool capturing = cudaStreamIsCapturing(stream, &cap) != cudaSuccess ||
+                         cap != cudaStreamCaptureStatusNone;
+  cudaGetLastError();  // a failed query leaves no sticky error behind
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_addr[dev] == nullptr) {
+  if (g_noalloc_addr[dev] == nullptr || !capturing) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_counters);
     if (e != cudaSuccess || p == nullptr)
@@ -92,7 +100,7 @@ extern "C" int fi_gpu_chunked_prefix_sum_noalloc_int64(
                      "Relation is too large and causes an integer overflow. Try "
                      "using more chunks by setting a higher CUDA grid size");
   uint32_t *scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
+  int rc = noalloc_scratch((cudaStream_t)stream, &scratch);
   if (rc) return rc;
   HistScratch s{scratch, nullptr, nullptr, nullptr};
   cudaError_t e = launch_chunked_prefix_sum<int64_t>(

@@ -256,11 +256,20 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         record_error(status, kDevErrTimeout);
-        if (t + 1 < ntiles) {  // bounded wait for the copy in flight
+        // Drain before the CTA's shared memory is released: wait (bounded)
+        // for both copies this CTA may still have in flight, tile t's (whose
+        // wait gave up) and tile t+1's.  A copy that outlasts these waits as
+        // well is reported by the timeout status above.
+        for (uint32_t round = 0; round < 4 && !mbar_wait(&bars[s], parity); ++round) {
+        }
+        if (t + 1 < ntiles) {
           const uint32_t s1 = (uint32_t)((t + 1) % S::kStages);
-          mbar_wait(&bars[s1], (uint32_t)(((t + 1) / S::kStages) & 1u));
+          const uint32_t p1 = (uint32_t)(((t + 1) / S::kStages) & 1u);
+          for (uint32_t round = 0; round < 4 && !mbar_wait(&bars[s1], p1); ++round) {
+          }
         }
       }
+      __syncthreads();
       return;
     }
     // 2. run offsets inside the tile

@@ -259,12 +259,15 @@ int fi_gpu_partition_int64(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
  * partitioner with grid = num_chunks, pass bits = radix_bits and
  * ignore_bits, but the scratch counters live in a fixed 2 MiB array inside
  * the library (held on every GPU that loads it until exit).  Limit:
- * num_chunks * 2^radix_bits <= 524288 counters, radix_bits <= 18; larger
- * requests fail with FI_ERR_INVALID_ARGUMENT.  The caller passes the keys
- * and the offsets buffer (num_chunks * 2^radix_bits u64).  All calls share
- * the array: calls that overlap on the GPU race; serialise them.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress), so
- * make it before capturing the stream into a graph. */
+ * num_chunks * 2^radix_bits <= 524288 counters (more fail with
+ * FI_ERR_INVALID_ARGUMENT) and radix_bits <= 18 (more fail with
+ * FI_ERR_UNSUPPORTED, as for every prefix sum of the library).  The caller
+ * passes the keys and the offsets buffer (num_chunks * 2^radix_bits u64).
+ * All calls share the array: calls that overlap on the GPU race; serialise
+ * them.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make it before capturing the stream into a
+ * graph; later calls outside a capture look it up again, so a
+ * cudaDeviceReset between calls is harmless. */
 int fi_gpu_chunked_prefix_sum_noalloc_int64(const int64_t *partition_attr,
                                             uint64_t len, uint32_t num_chunks,
                                             uint32_t radix_bits,

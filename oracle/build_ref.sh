@@ -8,10 +8,16 @@
 # lie.  The reference normally generates `constants.h` from
 # sql-ops/build.rs:74-120; this script writes the same values.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT
+#    or: FI_REFERENCE_ROOT=... oracle/build_ref.sh
+# Without either, or when the tree is absent, nothing is built.
 set -euo pipefail
 
-REF="${1:-/root/reference}"
+REF="${1:-${FI_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "build_ref: no reference root given; skipping" >&2
+  exit 0
+fi
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 SRC="$REF/sql-ops"

@@ -95,7 +95,7 @@ def run_partition(fi, oracle, keys, pays, tdt, hist, algo, grid, bits,
     return rel
 
 
-ALGOS = [fi_algo for fi_algo in ("NC", "SSWWCv2", "HSSWWCv4", "LASWWC")]
+ALGOS = ["NC", "SSWWCv2", "SSWWCv2G", "HSSWWCv4", "LASWWC"]
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)

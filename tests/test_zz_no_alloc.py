@@ -46,8 +46,13 @@ def test_noalloc_prefix_sum_matches_partitioner(fi, oracle):
     # two calls in a row with different inputs and shapes; both use the
     # shared scratch (few chunks, so several CTAs add into each chunk's
     # counters)
-    cases = [(1_000_003, 8, 10, 0, 1), (777_777, 5, 7, 3, 2)]
+    # 16 bits: two 2^15-bin range passes; 2 chunks x 18 bits: exactly the
+    # array's 524288 counters, filled by the thread-block-cluster histogram
+    cases = [(1_000_003, 8, 10, 0, 1), (777_777, 5, 7, 3, 2),
+             (600_001, 4, 16, 0, 3), (900_007, 2, 18, 0, 4),
+             (333_333, 3, 12, 5, 5)]
     for n, chunks, bits, ignore, seed in cases:
+        assert (chunks << bits) <= MAX_COUNTERS
         keys = torch.from_numpy(oracle.uniform_u64_keys(n, seed)).cuda()
         got = noalloc_offsets(fi, keys, chunks, bits, ignore)
         exp = reference_offsets(fi, keys, chunks, bits, ignore)
@@ -66,5 +71,11 @@ def test_noalloc_rejects_oversized_requests(fi):
         C.c_void_p(keys.data_ptr()), C.c_uint64(16), C.c_uint32(chunks),
         C.c_uint32(bits), C.c_uint32(0), C.c_void_p(out.data_ptr()),
         C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    assert rc == -1
+    assert rc == -1  # FI_ERR_INVALID_ARGUMENT
     assert b"exceeds the fixed scratch array" in fi.lib().fi_last_error()
+    # more radix bits than any prefix sum supports: FI_ERR_UNSUPPORTED
+    rc = fi.lib().fi_gpu_chunked_prefix_sum_noalloc_int64(
+        C.c_void_p(keys.data_ptr()), C.c_uint64(16), C.c_uint32(1),
+        C.c_uint32(19), C.c_uint32(0), C.c_void_p(out.data_ptr()),
+        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == -6
