@@ -56,11 +56,13 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
                     choices=["join", "partition", "ooc", "serve", "dataset", "nopart",
-                             "hybrid", "exchange"],
+                             "hybrid", "exchange", "refkernels"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
                          "join server against back-to-back plain calls; dataset: "
-                         "a named data set of the reference (--data-set)")
+                         "a named data set of the reference (--data-set); "
+                         "refkernels: the reference's own GPU kernels beside "
+                         "this repository's on the same inputs")
     ap.add_argument("--data-set", default="blanas",
                     choices=["blanas", "blanas4mb", "kim", "lutz2gv32g", "lutz32gv32g",
                              "custom"],
@@ -594,6 +596,178 @@ def run_partition_sweep(a):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_refkernels(a):
+    """The reference's own GPU kernels (baseline/refgpu: compiled for sm_100a
+    from its sources, launched with its argument structs, grids and shared
+    memory) beside this repository's on the same B200 and the same inputs.
+
+    Partition (config 2 shape): 2^part_log2n int64 tuples, uniform 64-bit
+    keys, SM-count chunks; per radix-bit setting the Chunked prefix sum and
+    the NC and LASWWC scatters of the reference against this repository's
+    prefix sum and scatter.  Every output is verified: offsets identical,
+    and each scattered relation checked region by region against its input.
+    The reference's SSWWC variants spin on buffer slots without a bound and
+    are not run.
+
+    Join: R = S = 2^24 int32 at 10 bits (config 1) and 2^28 int64 at 16 bits
+    (the final partitions of the config-3 join: ~4096 tuples each), keys a
+    seeded permutation of 1..N, uniform foreign keys, payload = key;
+    assign_tasks + the reference's shared-memory join (grid = SMs, 1024
+    threads) against this repository's join on the same partitioned
+    relations, both checked against the closed form (sum of S payloads)."""
+    import types
+    import torch
+    import fi_sqlops as fi
+    sys.path.insert(0, os.path.join(REPO, "baseline", "refgpu"))
+    import refgpu
+    world, rank, local = dist_setup(a.gpus)
+    if rank != 0:
+        return
+    if not refgpu.available():
+        print(json.dumps({"workload": "reference_gpu_kernels",
+                          "unavailable": "baseline/refgpu/_build/libref_gpu.so not built"}))
+        return
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    stream = torch.cuda.current_stream()
+    K, W = a.steps, max(a.warmup, 1)
+    peak, peak_kind = load_peaks()
+
+    def timed(fn):
+        for _ in range(W):
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True),
+                torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+
+    n = 1 << a.part_log2n
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    pays = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_uniform_u64_keys(keys, a.seed)
+    fi.gen_uniform_u64_keys(pays, a.seed + 1)
+    pad = fi.padding_len(torch.int64)
+    prows, jrows = [], []
+    with ClockSampler(local) as clk:
+        for bits in [int(b) for b in a.sweep.split(",") if int(b) <= 14]:
+            F = 1 << bits
+            row = {"radix_bits": bits}
+            ref_off = torch.empty(sms * F, dtype=torch.int64, device="cuda")
+            row["ref_prefix_sum_ms"] = timed(
+                lambda: refgpu.chunked_prefix_sum(keys, sms, bits, out=ref_off))
+            p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Chunked,
+                                       fi.GpuRadixPartitionAlgorithm.HSSWWCv4,
+                                       fi.RadixBits(bits), sms, 1024)
+            o = fi.PartitionOffsets(fi.GpuHistogramAlgorithm.Chunked, sms, bits,
+                                    torch.int64)
+            rel = fi.PartitionedRelation(n, fi.GpuHistogramAlgorithm.Chunked, bits, sms,
+                                         torch.int64)
+            row["our_prefix_sum_ms"] = timed(
+                lambda: p.prefix_sum(fi.RadixPass.First, keys, o))
+            row["offsets_identical"] = bool(torch.equal(o.offsets.view(-1), ref_off))
+
+            def ours_part():
+                p.prefix_sum(fi.RadixPass.First, keys, o)
+                p.partition(fi.RadixPass.First, keys, pays, o, rel)
+            both = timed(ours_part)
+            row["our_partition_ms"] = both - row["our_prefix_sum_ms"]
+            p.status()
+            row["our_verified"] = verify_partitioned(torch, keys, pays, rel, sms, bits, pad)
+            del p, o, rel
+            torch.cuda.empty_cache()
+            ref_rel = torch.empty((n + sms * F * pad, 2), dtype=torch.int64, device="cuda")
+            view = types.SimpleNamespace(offsets=ref_off, relation=ref_rel)
+            for name, variant in (("nc", refgpu.NC), ("laswwc", refgpu.LASWWC)):
+                try:
+                    part = refgpu.Partition(variant, keys, pays, sms, bits, ref_off,
+                                            ref_rel)
+                except refgpu.RefGpuError as e:
+                    row["ref_%s" % name] = "refused: %s" % e
+                    continue
+                row["ref_%s_partition_ms" % name] = timed(part.launch)
+                row["ref_%s_verified" % name] = verify_partitioned(
+                    torch, keys, pays, view, sms, bits, pad)
+            del ref_rel, view
+            torch.cuda.empty_cache()
+            row["ref_best_ms"] = row["ref_prefix_sum_ms"] + min(
+                v for k, v in row.items()
+                if k.startswith("ref_") and k.endswith("_partition_ms"))
+            row["our_ms"] = row["our_prefix_sum_ms"] + row["our_partition_ms"]
+            row["speedup"] = row["ref_best_ms"] / row["our_ms"]
+            row["our_gb_per_s"] = n * 40 / (row["our_ms"] / 1e3) / 1e9
+            row["ref_best_gb_per_s"] = n * 40 / (row["ref_best_ms"] / 1e3) / 1e9
+            prows.append(row)
+        del keys, pays
+        torch.cuda.empty_cache()
+        for label, dt, log2n, bits in (("config1_16Mx16M_int32_10bits", torch.int32, 24, 10),
+                                       ("final_partitions_256Mx256M_int64_16bits",
+                                        torch.int64, 28, 16)):
+            m = 1 << log2n
+            rk = torch.empty(m, dtype=dt, device="cuda")
+            sk = torch.empty(m, dtype=dt, device="cuda")
+            fi.gen_primary_keys(rk, a.seed + 7, base=1)
+            fi.gen_uniform_foreign_keys(sk, m, a.seed + 8, base=1)
+            exp = int(sk.to(torch.int64).sum().item()) & ((1 << 64) - 1)
+            rels = []
+            for k in (rk, sk):
+                pp = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Contiguous,
+                                            fi.GpuRadixPartitionAlgorithm.SSWWCv2,
+                                            fi.RadixBits(bits), sms, 1024)
+                oo = fi.PartitionOffsets(fi.GpuHistogramAlgorithm.Contiguous, sms, bits, dt)
+                rr = fi.PartitionedRelation(m, fi.GpuHistogramAlgorithm.Contiguous, bits,
+                                            sms, dt)
+                pp.prefix_sum(fi.RadixPass.First, k, oo)
+                pp.partition(fi.RadixPass.First, k, k, oo, rr)
+                pp.status()
+                rels.append(rr)
+            b, pr = rels
+            for sname, rscheme, fscheme in (("perfect", refgpu.PERFECT, fi.HashingScheme.Perfect),
+                                            ("chaining", refgpu.CHAINING,
+                                             fi.HashingScheme.BucketChaining)):
+                jr = {"workload": label, "scheme": sname, "tuples": 2 * m}
+                try:
+                    j = refgpu.Join(rscheme, b.relation, b.offsets, b.padded_len(),
+                                    pr.relation, pr.offsets, pr.padded_len(), bits,
+                                    bits, sms, 1024)
+                    j.launch()
+                    jr["ref_verified"] = j.sum() == exp
+                    jr["ref_join_ms"] = timed(j.launch)
+                except refgpu.RefGpuError as e:
+                    jr["ref"] = "refused: %s" % e
+                res = torch.zeros(sms * 1024, dtype=torch.int64, device="cuda")
+                tasks = torch.zeros(sms + 1, dtype=torch.int32, device="cuda")
+                jo = fi.CudaRadixJoin(fi.RadixPass.First, fi.RadixBits(bits), fscheme,
+                                      sms, 1024)
+                jo.join(b, pr, res, tasks)
+                jo.status()
+                jr["our_verified"] = (int(res.sum().item()) & ((1 << 64) - 1)) == exp
+                jr["our_join_ms"] = timed(lambda: jo.join(b, pr, res, tasks))
+                if "ref_join_ms" in jr:
+                    jr["speedup"] = jr["ref_join_ms"] / jr["our_join_ms"]
+                jrows.append(jr)
+            del rels, b, pr, rk, sk
+            torch.cuda.empty_cache()
+    line = {"metric": "reference GPU kernels vs this repository's (ms per launch)",
+            "workload": "reference_gpu_kernels", "n_gpus": 1, "steps": K,
+            "warmup": W, "dtype": "int64 / int32",
+            "data": "synthetic (uniform 64-bit keys; seeded permutation PK, uniform FK)",
+            "config": {"workload": "reference_gpu_kernels",
+                       "partition_tuples": n, "chunks": sms,
+                       "reference_grid_block": [sms, 1024]},
+            "peak": peak, "peak_source": peak_kind,
+            "partition": prows, "join": jrows, "clocks": clk.summary(),
+            "verified": all(r.get("offsets_identical") and r.get("our_verified")
+                            and all(v for k, v in r.items() if k.endswith("_verified"))
+                            for r in prows)
+            and all(all(v for k, v in r.items() if k.endswith("_verified"))
+                    for r in jrows)}
+    print(json.dumps(line), flush=True)
 
 
 def h2d_probe(torch, nbytes=1 << 30, reps=5):
@@ -1313,6 +1487,8 @@ def main():
         run_hybrid(a)
     elif a.workload == "exchange":
         run_exchange(a)
+    elif a.workload == "refkernels":
+        run_refkernels(a)
     else:
         run_ours(a)
 

@@ -126,3 +126,22 @@ def test_autotune_model_and_table(fi, tmp_path):
         fi.autotune_load(str(table))
     assert ex.value.kind == "InvalidArgument"
     fi.autotune_load(None)
+
+
+def test_reference_gpu_harness_exports():
+    """The launch harness of the reference's own GPU kernels
+    (baseline/refgpu) loads without a GPU and exports its entry points."""
+    import ctypes as C
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))), "baseline", "refgpu"))
+    import refgpu
+    if not refgpu.available():
+        pytest.skip("reference GPU kernels not built (no reference tree)")
+    lib = refgpu.lib()
+    for name in ("rg_chunked_prefix_sum", "rg_partition_prepare", "rg_partition",
+                 "rg_join_prepare", "rg_join", "rg_last_error", "rg_padding_len"):
+        assert hasattr(lib, name), name
+    assert lib.rg_padding_len(C.c_int(4)) == 16
+    assert lib.rg_padding_len(C.c_int(8)) == 8
