@@ -537,8 +537,8 @@ def run_partition_sweep(a):
     K = a.steps
     with ClockSampler(local) as clk:
         for bits in [int(b) for b in a.sweep.split(",")]:
-            # the reference's first-pass choice; the library uses one level
-            # up to 11 bits and two levels above
+            # the reference's first-pass choice; the library uses the tile
+            # scatter up to 11 bits and the wide scatter above
             p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Chunked,
                                        fi.GpuRadixPartitionAlgorithm.HSSWWCv4,
                                        fi.RadixBits(bits), chunks, 1024)
@@ -568,7 +568,8 @@ def run_partition_sweep(a):
             step_ms = max_over_ranks(hist_ms + part_ms, world)
             ok = verify_partitioned(torch, keys, pays, rel, chunks, bits, pad)
             gbs = world * n * 40 / (step_ms / 1e3) / 1e9
-            sweep.append({"radix_bits": bits, "scatter_levels": 1 if bits <= 11 else 2,
+            sweep.append({"radix_bits": bits,
+                          "scatter": "tile" if bits <= 11 else "wide",
                           "ms_per_step": step_ms, "prefix_sum_ms": hist_ms,
                           "partition_ms": part_ms, "gb_per_s": gbs,
                           "frac": gbs / world / peak,

@@ -522,14 +522,22 @@ extern "C" int fi_gpu_prefix_sum_and_transform_int64(
                                  dst_len, offsets, (cudaStream_t)stream);
 }
 
-// Whether a pass of `bits` uses the hierarchical two-level scatter: above
-// kSingleLevelBits for the write-combining algorithms, and above the
-// single-level limit for all (NC keeps one level while its per-partition
-// counters fit shared memory).
-static bool two_level(const fi_gpu_radix_partitioner *p, uint32_t bits) {
+// Whether a pass of `bits` leaves the tile scatter: above kSingleLevelBits
+// for the write-combining algorithms, and above the tile scatter's limit for
+// all (NC keeps its shared-memory counters while they fit).  Such passes use
+// the wide scatter (wide_scatter.cu), or with FI_HIERARCHICAL_SCATTER defined
+// the hierarchical two-level scatter it replaced.
+static bool high_fanout(const fi_gpu_radix_partitioner *p, uint32_t bits) {
   return bits > kMaxTileBits ||
          (bits > kSingleLevelBits && p->algo != FI_PARTITION_NC);
 }
+#ifdef FI_HIERARCHICAL_SCATTER
+static bool two_level(const fi_gpu_radix_partitioner *p, uint32_t bits) {
+  return high_fanout(p, bits);
+}
+#else
+static bool two_level(const fi_gpu_radix_partitioner *, uint32_t) { return false; }
+#endif
 
 template <typename K>
 static int preallocate_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass) {
@@ -622,6 +630,14 @@ static int partition_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
         keys, pays, len, chunks, bits, ignore, cursors, r->relation,
         r->relation_len, p->tmp_rel.ptr, (uint64_t *)p->tmp_cursors.ptr,
         p->hs(), device_sm_count(), stream);
+  } else if (high_fanout(p, bits)) {
+    // relative cursors in the histogram scratch, tile counter in the second
+    // word of the counter buffer (both idle once the prefix sum has run)
+    e = launch_partition_wide<K>(keys, pays, len, chunks, bits, ignore, cursors,
+                                 r->relation, r->relation_len,
+                                 (uint32_t *)p->hist_buf.ptr,
+                                 (uint32_t *)p->counter.ptr + 1,
+                                 (int *)p->status.ptr, device_sm_count(), stream);
   } else {
     e = launch_partition<K>(keys, pays, len, chunks, bits, ignore, cursors,
                             r->relation, r->relation_len,

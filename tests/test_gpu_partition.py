@@ -162,8 +162,8 @@ def test_partition_unaligned_columns(fi, oracle, ndt, tdt, bits):
                                             ("Contiguous", 16, 8),
                                             ("Contiguous", 18, 3)])
 def test_partition_hierarchical(fi, oracle, ndt, tdt, hist, bits, grid):
-    """Fanouts above the single-level tile scatter (2^15..2^18, the
-    partition sweep's "hierarchical" fanouts) use the two-level scatter."""
+    """Fanouts above the tile scatter (2^15..2^18, the partition sweep's
+    "hierarchical" fanouts of the reference) use the wide scatter."""
     n = 1 << 20
     keys, pays = gen(oracle, n, ndt, 5, kind="u64")
     H = getattr(fi.GpuHistogramAlgorithm, hist)
@@ -182,6 +182,36 @@ def test_partition_hierarchical(fi, oracle, ndt, tdt, hist, bits, grid):
     assert_same_partitions(got, ref, off, chunks, bits, padded,
                            oracle.padding_len(ndt))
     assert (got[:, 0] != -1).sum() == n
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("hist", ["Chunked", "Contiguous"])
+@pytest.mark.parametrize("n,grid,bits,kind", [(5000, 37, 12, "u64"),
+                                              (20000, 148, 13, "u64"),
+                                              (1 << 20, 148, 12, "zipf"),
+                                              (300001, 7, 18, "zipf"),
+                                              (1 << 20, 148, 16, "u64"),
+                                              (999999, 64, 17, "u64")])
+def test_partition_wide(fi, oracle, ndt, tdt, hist, n, grid, bits, kind):
+    """The single-level wide scatter above 11 bits (and the wide histogram
+    from 17 bits): tiles that span several small chunks, Zipf-skewed keys
+    whose lanes share (chunk, partition) cursors, Contiguous per-block
+    cursors, up to 2^18 partitions."""
+    keys, pays = gen(oracle, n, ndt, 9, kind=kind)
+    H = getattr(fi.GpuHistogramAlgorithm, hist)
+    rel = run_partition(fi, oracle, keys, pays, tdt, H,
+                        fi.GpuRadixPartitionAlgorithm.SSWWCv2, grid, bits)
+    if hist == "Chunked":
+        off = oracle.chunked_prefix_sum(keys, grid, bits)
+        cursors, chunks = off, grid
+    else:
+        off, cursors = oracle.contiguous_prefix_sum(keys, grid, bits)
+        chunks = 1
+    np.testing.assert_array_equal(to_host(rel.offsets).astype(np.uint64), off)
+    padded = rel.padded_len()
+    ref = oracle.chunked_radix_partition(keys, pays, cursors, grid, bits, 0, padded)
+    assert_same_partitions(to_host(rel.relation)[:padded], ref, off, chunks, bits,
+                           padded, oracle.padding_len(ndt))
 
 
 @pytest.mark.parametrize("algo", ["NC", "SSWWCv2"])
