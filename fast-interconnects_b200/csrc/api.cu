@@ -525,8 +525,8 @@ extern "C" int fi_gpu_prefix_sum_and_transform_int64(
 // Whether a pass of `bits` leaves the tile scatter: above kSingleLevelBits
 // for the write-combining algorithms, and above the tile scatter's limit for
 // all (NC keeps its shared-memory counters while they fit).  Such passes use
-// the wide scatter (wide_scatter.cu), or with FI_HIERARCHICAL_SCATTER defined
-// the hierarchical two-level scatter it replaced.
+// the pipelined two-level scatter (pipelined_scatter.cu), or with
+// FI_HIERARCHICAL_SCATTER defined the unpipelined two-level scatter.
 static bool high_fanout(const fi_gpu_radix_partitioner *p, uint32_t bits) {
   return bits > kMaxTileBits ||
          (bits > kSingleLevelBits && p->algo != FI_PARTITION_NC);
@@ -548,6 +548,9 @@ static int preallocate_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass) {
   if (two_level(p, bits)) {
     const uint32_t hi = hierarchical_hi_bits(bits);
     rc = p->tmp_cursors.reserve(((size_t)p->grid << hi) * sizeof(uint64_t), false);
+    if (rc) return rc;
+  } else if (high_fanout(p, bits)) {
+    rc = p->tmp_cursors.reserve(pipelined_scatter_work_bytes(p->grid, bits), false);
     if (rc) return rc;
   }
   return p->scratch(1u << std::min(bits, kMaxHistBits), p->grid);
@@ -631,13 +634,14 @@ static int partition_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
         r->relation_len, p->tmp_rel.ptr, (uint64_t *)p->tmp_cursors.ptr,
         p->hs(), device_sm_count(), stream);
   } else if (high_fanout(p, bits)) {
-    // relative cursors in the histogram scratch, tile counter in the second
-    // word of the counter buffer (both idle once the prefix sum has run)
-    e = launch_partition_wide<K>(keys, pays, len, chunks, bits, ignore, cursors,
-                                 r->relation, r->relation_len,
-                                 (uint32_t *)p->hist_buf.ptr,
-                                 (uint32_t *)p->counter.ptr + 1,
-                                 (int *)p->status.ptr, device_sm_count(), stream);
+    rc = p->tmp_cursors.reserve(pipelined_scatter_work_bytes(chunks, bits), false);
+    if (rc) return rc;
+    rc = p->tmp_rel.reserve((size_t)len * 2 * sizeof(K), false);
+    if (rc) return rc;
+    e = launch_partition_pipelined<K>(
+        keys, pays, len, chunks, bits, ignore, cursors, contiguous,
+        rel_padded_len(r), r->relation, r->relation_len, p->tmp_rel.ptr,
+        p->tmp_cursors.ptr, (int *)p->status.ptr, device_sm_count(), stream);
   } else {
     e = launch_partition<K>(keys, pays, len, chunks, bits, ignore, cursors,
                             r->relation, r->relation_len,

@@ -89,36 +89,19 @@ cudaError_t launch_partition_hierarchical(
     HistScratch s, uint32_t sm_count, cudaStream_t stream);
 uint32_t hierarchical_hi_bits(uint32_t radix_bits);
 
-// Single-level scatter for high fanouts (wide_scatter.cu): all CTAs walk the
-// input in tile order and claim each tuple's slot with a global atomic on
-// its (chunk, partition) cursor.  rel_cursors: chunks * 2^radix_bits u32 of
-// scratch; tile_counter: one u32.
+// Pipelined two-level scatter for high fanouts (pipelined_scatter.cu).
+// Level 1 sorts tiles of a chunk by the high half of the radix bits into
+// per-(chunk, bucket) ranges of `tmp` (len tuples); level 2 scatters each
+// bucket by the low half into the final slots, right after its chunk's
+// level 1, so that it reads level 1's output from L2.  `work` holds
+// pipelined_scatter_work_bytes(chunks, radix_bits) of scratch.
+size_t pipelined_scatter_work_bytes(uint32_t chunks, uint32_t radix_bits);
 template <typename K>
-cudaError_t launch_partition_wide(const K *keys, const K *pays, uint64_t len,
-                                  uint32_t chunks, uint32_t radix_bits,
-                                  uint32_t ignore_bits, const uint64_t *cursors,
-                                  void *out, uint64_t out_len,
-                                  uint32_t *rel_cursors, uint32_t *tile_counter,
-                                  int *status, uint32_t sm_count,
-                                  cudaStream_t stream);
-
-// The Chunked prefix sum counts with launch_wide_chunk_histogram from this
-// many radix bits on (when its scratch has a tile counter).
-#ifndef FI_WIDE_HIST_MIN_BITS
-#define FI_WIDE_HIST_MIN_BITS 17
-#endif
-constexpr uint32_t kWideHistMinBits = FI_WIDE_HIST_MIN_BITS;
-
-// Per-chunk histograms (hist: chunks * 2^radix_bits u32, zeroed by the
-// caller) by one warp-aggregated global reduction per tuple, tiles in input
-// order so that only one or two chunks' histograms are hot in L2.
-template <typename K>
-cudaError_t launch_wide_chunk_histogram(const K *keys, uint64_t len,
-                                        uint64_t clen, uint32_t chunks,
-                                        uint32_t radix_bits,
-                                        uint32_t ignore_bits, uint32_t *hist,
-                                        uint32_t *tile_counter,
-                                        uint32_t sm_count, cudaStream_t stream);
+cudaError_t launch_partition_pipelined(
+    const K *keys, const K *pays, uint64_t len, uint32_t chunks,
+    uint32_t radix_bits, uint32_t ignore_bits, const uint64_t *cursors,
+    bool contiguous, uint64_t padded_len, void *out, uint64_t out_len,
+    void *tmp, void *work, int *status, uint32_t sm_count, cudaStream_t stream);
 
 // ---- radix join ---------------------------------------------------------
 struct JoinScratch {

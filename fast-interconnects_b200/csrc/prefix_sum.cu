@@ -537,11 +537,7 @@ cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
   }
   e = cudaMemsetAsync(s.hist, 0, (size_t)chunks * F * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  if (radix_bits >= kWideHistMinBits && s.tile_counter != nullptr) {
-    e = launch_wide_chunk_histogram<K>(keys, len, clen, chunks, radix_bits,
-                                       ignore_bits, s.hist, s.tile_counter,
-                                       sm_count, stream);
-  } else if (ranges > 1) {
+  if (ranges > 1) {
     e = launch_wide_histogram<K>(keys, nullptr, nullptr, nullptr, len, clen,
                                  chunks, splits, radix_bits, ignore_bits, pad,
                                  s.hist, stream);

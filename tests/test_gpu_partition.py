@@ -191,12 +191,12 @@ def test_partition_hierarchical(fi, oracle, ndt, tdt, hist, bits, grid):
                                               (1 << 20, 148, 12, "zipf"),
                                               (300001, 7, 18, "zipf"),
                                               (1 << 20, 148, 16, "u64"),
-                                              (999999, 64, 17, "u64")])
-def test_partition_wide(fi, oracle, ndt, tdt, hist, n, grid, bits, kind):
-    """The single-level wide scatter above 11 bits (and the wide histogram
-    from 17 bits): tiles that span several small chunks, Zipf-skewed keys
-    whose lanes share (chunk, partition) cursors, Contiguous per-block
-    cursors, up to 2^18 partitions."""
+                                              (999999, 64, 17, "u64"),
+                                              (3000, 200, 12, "u64")])
+def test_partition_high_fanout(fi, oracle, ndt, tdt, hist, n, grid, bits, kind):
+    """The pipelined two-level scatter above 11 bits: tiles that span several
+    small chunks (or chunks of length 0), Zipf-skewed keys filling a few
+    buckets, Contiguous per-block cursors, up to 2^18 partitions."""
     keys, pays = gen(oracle, n, ndt, 9, kind=kind)
     H = getattr(fi.GpuHistogramAlgorithm, hist)
     rel = run_partition(fi, oracle, keys, pays, tdt, H,
