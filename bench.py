@@ -538,7 +538,7 @@ def run_partition_sweep(a):
     with ClockSampler(local) as clk:
         for bits in [int(b) for b in a.sweep.split(",")]:
             # the reference's first-pass choice; the library uses the tile
-            # scatter up to 11 bits and the wide scatter above
+            # scatter up to 11 bits and the two-level scatter above
             p = fi.GpuRadixPartitioner(fi.GpuHistogramAlgorithm.Chunked,
                                        fi.GpuRadixPartitionAlgorithm.HSSWWCv4,
                                        fi.RadixBits(bits), chunks, 1024)
@@ -569,7 +569,7 @@ def run_partition_sweep(a):
             ok = verify_partitioned(torch, keys, pays, rel, chunks, bits, pad)
             gbs = world * n * 40 / (step_ms / 1e3) / 1e9
             sweep.append({"radix_bits": bits,
-                          "scatter": "tile" if bits <= 11 else "wide",
+                          "scatter": "tile" if bits <= 11 else "two-level",
                           "ms_per_step": step_ms, "prefix_sum_ms": hist_ms,
                           "partition_ms": part_ms, "gb_per_s": gbs,
                           "frac": gbs / world / peak,

@@ -522,22 +522,14 @@ extern "C" int fi_gpu_prefix_sum_and_transform_int64(
                                  dst_len, offsets, (cudaStream_t)stream);
 }
 
-// Whether a pass of `bits` leaves the tile scatter: above kSingleLevelBits
-// for the write-combining algorithms, and above the tile scatter's limit for
-// all (NC keeps its shared-memory counters while they fit).  Such passes use
-// the pipelined two-level scatter (pipelined_scatter.cu), or with
-// FI_HIERARCHICAL_SCATTER defined the unpipelined two-level scatter.
-static bool high_fanout(const fi_gpu_radix_partitioner *p, uint32_t bits) {
+// Whether a pass of `bits` uses the hierarchical two-level scatter: above
+// kSingleLevelBits for the write-combining algorithms, and above the
+// single-level limit for all (NC keeps one level while its per-partition
+// counters fit shared memory).
+static bool two_level(const fi_gpu_radix_partitioner *p, uint32_t bits) {
   return bits > kMaxTileBits ||
          (bits > kSingleLevelBits && p->algo != FI_PARTITION_NC);
 }
-#ifdef FI_HIERARCHICAL_SCATTER
-static bool two_level(const fi_gpu_radix_partitioner *p, uint32_t bits) {
-  return high_fanout(p, bits);
-}
-#else
-static bool two_level(const fi_gpu_radix_partitioner *, uint32_t) { return false; }
-#endif
 
 template <typename K>
 static int preallocate_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass) {
@@ -548,9 +540,6 @@ static int preallocate_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass) {
   if (two_level(p, bits)) {
     const uint32_t hi = hierarchical_hi_bits(bits);
     rc = p->tmp_cursors.reserve(((size_t)p->grid << hi) * sizeof(uint64_t), false);
-    if (rc) return rc;
-  } else if (high_fanout(p, bits)) {
-    rc = p->tmp_cursors.reserve(pipelined_scatter_work_bytes(p->grid, bits), false);
     if (rc) return rc;
   }
   return p->scratch(1u << std::min(bits, kMaxHistBits), p->grid);
@@ -630,18 +619,9 @@ static int partition_impl(fi_gpu_radix_partitioner *p, fi_radix_pass pass,
     rc = p->tmp_rel.reserve((size_t)len * 2 * sizeof(K), false);
     if (rc) return rc;
     e = launch_partition_hierarchical<K>(
-        keys, pays, len, chunks, bits, ignore, cursors, r->relation,
-        r->relation_len, p->tmp_rel.ptr, (uint64_t *)p->tmp_cursors.ptr,
-        p->hs(), device_sm_count(), stream);
-  } else if (high_fanout(p, bits)) {
-    rc = p->tmp_cursors.reserve(pipelined_scatter_work_bytes(chunks, bits), false);
-    if (rc) return rc;
-    rc = p->tmp_rel.reserve((size_t)len * 2 * sizeof(K), false);
-    if (rc) return rc;
-    e = launch_partition_pipelined<K>(
         keys, pays, len, chunks, bits, ignore, cursors, contiguous,
         rel_padded_len(r), r->relation, r->relation_len, p->tmp_rel.ptr,
-        p->tmp_cursors.ptr, (int *)p->status.ptr, device_sm_count(), stream);
+        (uint64_t *)p->tmp_cursors.ptr, p->hs(), device_sm_count(), stream);
   } else {
     e = launch_partition<K>(keys, pays, len, chunks, bits, ignore, cursors,
                             r->relation, r->relation_len,

@@ -80,28 +80,18 @@ cudaError_t launch_partition(const K *keys, const K *pays, uint64_t len,
 // Hierarchical (two-level) scatter for large fanouts: level 1 scatters by the
 // high half of the pass bits into `tmp` (same chunking), level 2 scatters
 // every (chunk, high bucket) by the low half into `out`.  tmp_cursors holds
-// chunks * 2^hi_bits u64; tmp holds len + chunks*2^hi_bits*pad tuples.
+// chunks * 2^hi_bits u64; tmp holds len tuples.  The level-1 layout comes
+// from the final cursors (Chunked offsets, or Contiguous per-block cursors
+// when `contiguous`; padded_len is the relation's padded length).
 template <typename K>
 cudaError_t launch_partition_hierarchical(
     const K *keys, const K *pays, uint64_t len, uint32_t chunks,
     uint32_t radix_bits, uint32_t ignore_bits, const uint64_t *cursors,
-    void *out, uint64_t out_len, void *tmp, uint64_t *tmp_cursors,
-    HistScratch s, uint32_t sm_count, cudaStream_t stream);
+    bool contiguous, uint64_t padded_len, void *out, uint64_t out_len,
+    void *tmp, uint64_t *tmp_cursors, HistScratch s, uint32_t sm_count,
+    cudaStream_t stream);
 uint32_t hierarchical_hi_bits(uint32_t radix_bits);
 
-// Pipelined two-level scatter for high fanouts (pipelined_scatter.cu).
-// Level 1 sorts tiles of a chunk by the high half of the radix bits into
-// per-(chunk, bucket) ranges of `tmp` (len tuples); level 2 scatters each
-// bucket by the low half into the final slots, right after its chunk's
-// level 1, so that it reads level 1's output from L2.  `work` holds
-// pipelined_scatter_work_bytes(chunks, radix_bits) of scratch.
-size_t pipelined_scatter_work_bytes(uint32_t chunks, uint32_t radix_bits);
-template <typename K>
-cudaError_t launch_partition_pipelined(
-    const K *keys, const K *pays, uint64_t len, uint32_t chunks,
-    uint32_t radix_bits, uint32_t ignore_bits, const uint64_t *cursors,
-    bool contiguous, uint64_t padded_len, void *out, uint64_t out_len,
-    void *tmp, void *work, int *status, uint32_t sm_count, cudaStream_t stream);
 
 // ---- radix join ---------------------------------------------------------
 struct JoinScratch {

@@ -171,6 +171,59 @@ __global__ void __launch_bounds__(S::kThreads, S::kMinBlocks)
 
 uint32_t hierarchical_hi_bits(uint32_t radix_bits) { return (radix_bits + 1) / 2; }
 
+// Tuples of final region (c, p) under the cursor layout: Chunked offsets
+// (region (c, p) ends where (c, p+1) starts minus padding, a chunk's last
+// region where the next chunk's first starts minus padding, the relation's
+// last at its padded length), or Contiguous per-block cursors (block c's
+// share of partition p ends where block c+1's share starts; the last
+// block's where partition p+1 starts minus padding).
+__device__ __forceinline__ uint64_t region_len(const uint64_t *cur, uint32_t c,
+                                               uint32_t p, uint32_t chunks,
+                                               uint32_t F, uint32_t pad,
+                                               bool contiguous,
+                                               uint64_t padded_len) {
+  const uint64_t i = (uint64_t)c * F + p;
+  uint64_t next;
+  if (contiguous) {
+    if (c + 1 < chunks)
+      next = cur[i + F];
+    else
+      next = (p + 1 < F) ? cur[p + 1] - pad : padded_len;
+  } else {
+    next = (p + 1 < F || c + 1 < chunks) ? cur[i + 1] - pad : padded_len;
+  }
+  return next - cur[i];
+}
+
+// Level-1 layout of the hierarchical scatter from the final cursors, one CTA
+// per chunk: high bucket h of chunk c (the final regions (c, h*FL) ..
+// (c, h*FL + FL - 1)) starts at c * clen + the tuples of the chunk's buckets
+// before it, so a chunk's buckets fill its input range of `tmp`.  Replaces a
+// second histogram pass over the keys.
+__global__ void hierarchical_layout_kernel(const uint64_t *__restrict__ cursors,
+                                           uint32_t chunks, uint32_t radix_bits,
+                                           uint32_t hi, uint32_t pad,
+                                           bool contiguous, uint64_t padded_len,
+                                           uint64_t clen,
+                                           uint64_t *__restrict__ tmp_cursors) {
+  __shared__ uint64_t scan[33];
+  const uint32_t c = blockIdx.x, F = 1u << radix_bits, FH = 1u << hi;
+  const uint32_t FL = F >> hi;
+  uint64_t run = (uint64_t)c * clen;
+  for (uint32_t h0 = 0; h0 < FH; h0 += blockDim.x) {
+    const uint32_t h = h0 + threadIdx.x;
+    uint64_t n = 0;
+    if (h < FH)
+      for (uint32_t l = 0; l < FL; ++l)
+        n += region_len(cursors, c, h * FL + l, chunks, F, pad, contiguous,
+                        padded_len);
+    uint64_t total;
+    const uint64_t ex = block_exclusive_scan_u64(n, scan, &total);
+    if (h < FH) tmp_cursors[(uint64_t)c * FH + h] = run + ex;
+    run += total;
+  }
+}
+
 template <typename K, typename S>
 static cudaError_t launch_tile_shape(const K *keys, const K *pays, uint64_t len,
                                      uint64_t clen, uint32_t chunks,
@@ -248,15 +301,19 @@ template <typename K>
 cudaError_t launch_partition_hierarchical(
     const K *keys, const K *pays, uint64_t len, uint32_t chunks,
     uint32_t radix_bits, uint32_t ignore_bits, const uint64_t *cursors,
-    void *out, uint64_t out_len, void *tmp, uint64_t *tmp_cursors,
-    HistScratch s, uint32_t sm_count, cudaStream_t stream) {
+    bool contiguous, uint64_t padded_len, void *out, uint64_t out_len,
+    void *tmp, uint64_t *tmp_cursors, HistScratch s, uint32_t sm_count,
+    cudaStream_t stream) {
   using S = TileWide<K>;
   const uint32_t hi = hierarchical_hi_bits(radix_bits), lo = radix_bits - hi;
   // level-1 layout: same canonical chunks, partitions by the high bits, no
-  // padding
-  cudaError_t e = launch_chunked_prefix_sum<K>(keys, len, chunks, hi,
-                                               ignore_bits + lo, 0u,
-                                               tmp_cursors, s, sm_count, stream);
+  // padding; bucket sizes are sums of the final regions' sizes
+  constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+  const uint64_t clen = ((len + chunks - 1) / chunks) & kAlignMask;
+  hierarchical_layout_kernel<<<chunks, 256, 0, stream>>>(
+      cursors, chunks, radix_bits, hi, (uint32_t)(kPaddingBytes / sizeof(Tuple<K>)),
+      contiguous, padded_len, clen, tmp_cursors);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   e = launch_tile<K>(keys, pays, len, chunks, hi, ignore_bits + lo,
                      tmp_cursors, tmp, len, s.status, stream);
@@ -279,8 +336,8 @@ cudaError_t launch_partition_hierarchical(
       const uint64_t *, void *, uint64_t, int, int *, cudaStream_t);           \
   template cudaError_t launch_partition_hierarchical<K>(                       \
       const K *, const K *, uint64_t, uint32_t, uint32_t, uint32_t,            \
-      const uint64_t *, void *, uint64_t, void *, uint64_t *, HistScratch,     \
-      uint32_t, cudaStream_t);
+      const uint64_t *, bool, uint64_t, void *, uint64_t, void *, uint64_t *,  \
+      HistScratch, uint32_t, cudaStream_t);
 
 FI_INSTANTIATE_PARTITION(int32_t)
 FI_INSTANTIATE_PARTITION(int64_t)

@@ -194,9 +194,10 @@ def test_partition_hierarchical(fi, oracle, ndt, tdt, hist, bits, grid):
                                               (999999, 64, 17, "u64"),
                                               (3000, 200, 12, "u64")])
 def test_partition_high_fanout(fi, oracle, ndt, tdt, hist, n, grid, bits, kind):
-    """The pipelined two-level scatter above 11 bits: tiles that span several
-    small chunks (or chunks of length 0), Zipf-skewed keys filling a few
-    buckets, Contiguous per-block cursors, up to 2^18 partitions."""
+    """The two-level scatter above 11 bits, whose level-1 layout comes from
+    the final cursors: tiles that span several small chunks (or chunks of
+    length 0), Zipf-skewed keys filling a few buckets, Contiguous per-block
+    cursors, up to 2^18 partitions."""
     keys, pays = gen(oracle, n, ndt, 9, kind=kind)
     H = getattr(fi.GpuHistogramAlgorithm, hist)
     rel = run_partition(fi, oracle, keys, pays, tdt, H,
