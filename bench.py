@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--workload", default="join",
                     choices=["join", "partition", "ooc", "serve", "dataset", "nopart",
-                             "hybrid", "exchange", "refkernels"],
+                             "hybrid", "exchange", "refkernels", "sharded"],
                     help="partition: the partition-only sweep; ooc: the "
                          "out-of-core join from pinned host memory; serve: the "
                          "join server against back-to-back plain calls; dataset: "
@@ -87,6 +87,14 @@ def parse():
     ap.add_argument("--exchange-log2n", type=int, default=29,
                     help="exchange workload: int64 tuples one sender partitions "
                          "and sends")
+    ap.add_argument("--exchange", default="peer", choices=["peer", "nccl"],
+                    help="sharded workload: fused peer-store exchange or the "
+                         "library partition + NCCL all-to-all")
+    ap.add_argument("--emulate-ranks", type=int, default=1,
+                    help="sharded workload on one GPU: ranks emulated in one process")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 GPUs: N independent replicas of the join "
+                         "instead of the sharded join")
     ap.add_argument("--exchange-ranks", type=int, default=8,
                     help="exchange workload: receivers (power of two), emulated "
                          "by local receive columns on this GPU")
@@ -596,6 +604,195 @@ def run_partition_sweep(a):
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def sharded_relations(fi, torch, D, n, world, rank, seed):
+    """Rank `rank`'s shards: R = n primary keys, a seeded permutation spread
+    over the ranks (distributed.shard_primary_keys: all ranks' shards make a
+    permutation of 1..world*n); S = n foreign keys uniform over 1..world*n
+    with a seed per rank; payload = key."""
+    rk = torch.empty(n, dtype=torch.int64, device="cuda")
+    sk = torch.empty(n, dtype=torch.int64, device="cuda")
+    fi.gen_primary_keys(rk, seed, base=1)
+    D.shard_primary_keys(rk, world, rank)
+    fi.gen_uniform_foreign_keys(sk, world * n, seed + 1 + rank, base=1)
+    return rk, sk
+
+
+def run_sharded(a):
+    """The join of R and S sharded over the ranks (the default for N > 1):
+    each rank holds 2^log2n tuples of R and of S (weak scaling), sends every
+    tuple to the rank named by the key bits above the local join's with the
+    fused partition + peer-store kernel (distributed.PeerExchange, CUDA IPC
+    receive columns; --exchange nccl: library partition + NCCL all-to-all),
+    joins what it received with one reused engine, and an all-reduce adds
+    the ranks' {sum, count}.  value = all ranks' tuples / the step's device
+    time, max over ranks.  Checked against the closed form (every S key is a
+    foreign key: count = world * n, sum = sum of all S payloads).
+
+    With one GPU and --emulate-ranks W > 1 the W ranks are emulated in one
+    process: every emulated sender's fused scatter writes into the W local
+    receive columns, one after another, then the W local joins run; the
+    value is all tuples / the whole time on the one GPU."""
+    import torch
+    import torch.distributed as dist
+    import fi_sqlops as fi
+    import distributed as D
+    world, rank, local = dist_setup(a.gpus)
+    n = 1 << a.log2n
+    bits = tuple(int(b) for b in a.bits.split(","))
+    scheme = (fi.HashingScheme.Perfect if a.scheme == "perfect"
+              else fi.HashingScheme.BucketChaining)
+    stream = torch.cuda.current_stream()
+    emulate = a.emulate_ranks if world == 1 else 1
+    W = max(world, emulate)
+    shift = sum(bits)
+    g = D.exchange_bits(W)
+    mask = (1 << 64) - 1
+    K = a.steps
+
+    if emulate > 1:
+        m = n // emulate
+        shards = [sharded_relations(fi, torch, D, m, emulate, r, a.seed) for r in range(emulate)]
+        expected = (sum(int(sk.sum().item()) for _, sk in shards) & mask, emulate * m)
+        mats = []
+        for rel in (0, 1):
+            mats.append(torch.stack([fi.exchange_histogram(sh[rel], shift, g)
+                                     for sh in shards]).cpu())
+        recv = [m_.sum(0).tolist() for m_ in mats]
+        cols = [[torch.empty((2, max(c, 1)), dtype=torch.int64, device="cuda")
+                 for c in recv[rel]] for rel in (0, 1)]
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        engine = D.EngineJoin(max(recv[0]), max(recv[1]), torch.int64, bits, scheme)
+
+        def step():
+            for rel in (0, 1):
+                for s_, sh in enumerate(shards):
+                    base, _ = D.region_bases(mats[rel], s_)
+                    dests = [(cols[rel][d][0].data_ptr(), cols[rel][d][1].data_ptr(),
+                              base[d], recv[rel][d]) for d in range(W)]
+                    fi.exchange_scatter(sh[rel], sh[rel], shift, g, dests, status=status)
+            tot_s, tot_c = 0, 0
+            for d in range(W):
+                nr, ns = recv[0][d], recv[1][d]
+                if nr and ns:
+                    sm_, c_ = engine(cols[0][d][0][:nr], cols[0][d][1][:nr],
+                                     cols[1][d][0][:ns], cols[1][d][1][:ns], bits, scheme)
+                    tot_s, tot_c = (tot_s + sm_) & mask, tot_c + c_
+            return tot_s, tot_c
+        ex_ms = None
+    else:
+        rk, sk = sharded_relations(fi, torch, D, n, world, rank, a.seed)
+        part = torch.tensor([int(sk.sum().item())], dtype=torch.int64, device="cuda")
+        if world > 1:
+            dist.all_reduce(part)
+        expected = (int(part.item()) & mask, world * n)
+        caps = [max(D.region_bases(D.all_gather_counts(
+            fi.exchange_histogram(k, shift, g)), rank)[1]) for k in (rk, sk)]
+        peers = None
+        if a.exchange == "peer":
+            peers = (D.PeerExchange(caps[0], torch.int64), D.PeerExchange(caps[1], torch.int64))
+        engine = D.EngineJoin(caps[0], caps[1], torch.int64, bits, scheme)
+        ev_x = []
+
+        def step():
+            # exchange_join's steps, with events around the two shuffles
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if peers is not None:
+                rk2, rp2 = peers[0].shuffle(rk, rk, shift)
+                sk2, sp2 = peers[1].shuffle(sk, sk, shift)
+            else:
+                rk2, rp2 = D.shuffle(rk, rk, shift)
+                sk2, sp2 = D.shuffle(sk, sk, shift)
+            e1.record(stream)
+            ev_x.append((e0, e1))
+            s_, c_ = engine(rk2, rp2, sk2, sp2, bits, scheme)
+            tt = torch.tensor([s_, c_], dtype=torch.int64, device="cuda")
+            if world > 1:
+                dist.all_reduce(tt)
+            return int(tt[0].item()) & mask, int(tt[1].item())
+
+    verified = True
+    for _ in range(max(a.warmup, 1)):
+        verified = verified and step() == expected
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if emulate == 1:
+        ev_x.clear()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(K):
+            verified = step() == expected and verified
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_per_step = max_over_ranks(ev0.elapsed_time(ev1) / K, world)
+    value = 2 * W * (n if emulate == 1 else n // emulate) / (ms_per_step / 1e3) / 1e9
+    clocks = clk.summary()
+    nvlink = None
+    if emulate == 1:
+        ex_ms = max_over_ranks(statistics.mean(a_.elapsed_time(b_) for a_, b_ in ev_x), world)
+        sent = 2 * n * 16 * (W - 1) / W  # tuples leaving this rank, both relations
+        nvlink = {"exchange_ms": ex_ms, "bytes_sent_per_rank": int(sent),
+                  "achieved_gb_per_s": sent / (ex_ms / 1e3) / 1e9 if W > 1 else None,
+                  "peak_gb_per_s": 770.0, "peak_source": "measured peer copy per direction"}
+
+    e2e = None
+    if emulate == 1 and not a.no_e2e and a.e2e_steps > 0:
+        # the public API with host columns: H2D copies of this rank's four
+        # columns, exchange_join, result back to the host
+        host = [torch.empty(n, dtype=torch.int64, pin_memory=True) for _ in range(4)]
+        for h, d in zip(host, (rk, rk, sk, sk)):
+            h.copy_(d)
+        rp_d, sp_d = torch.empty_like(rk), torch.empty_like(sk)
+        t_e2e = []
+        for _ in range(a.e2e_steps):
+            barrier(world)
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for dst, h in zip((rk, rp_d, sk, sp_d), host):
+                dst.copy_(h, non_blocking=True)
+            res = D.exchange_join(rk, rp_d, sk, sp_d, bits=bits, scheme=scheme,
+                                  exchange=a.exchange, peers=peers, local_join=engine)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            verified = verified and ((res[0] & mask), res[1]) == expected
+            t_e2e.append(t0.elapsed_time(t1))
+        e2e_ms = max_over_ranks(statistics.mean(t_e2e), world)
+        e2e = {"value": 2 * world * n / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n * 8 * world, "d2h_bytes_per_step": 16 * world,
+               "ms_per_step": e2e_ms,
+               "path": "distributed.exchange_join over pinned host columns copied in per step"}
+        del host
+    if emulate == 1 and peers is not None:
+        for p_ in peers:
+            p_.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": K, "warmup": a.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int64",
+                "data": "synthetic (seeded permutation PK spread over the ranks, "
+                        "uniform FK over all ranks' keys, payload = key)",
+                "config": {"workload": "sharded_radix_join_%dx(%dMx%dM)_int64_%sbits_%s"
+                                       % (W, (n // emulate) >> 20, (n // emulate) >> 20,
+                                          "+".join(map(str, bits)), a.scheme),
+                           "tuples_per_rank_per_relation": n // emulate,
+                           "ranks": W, "emulated_ranks": emulate > 1,
+                           "exchange": "emulated local receive columns" if emulate > 1
+                                       else a.exchange,
+                           "exchange_bits": g, "radix_bits": list(bits),
+                           "l2_flush": "none: inputs larger than L2",
+                           "parallelism": "sharded%d" % W},
+                "nvlink": nvlink, "e2e": e2e, "clocks": clocks,
+                "verified": bool(verified)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
         dist.destroy_process_group()
 
 
@@ -1490,6 +1687,9 @@ def main():
         run_exchange(a)
     elif a.workload == "refkernels":
         run_refkernels(a)
+    elif a.workload == "sharded" or (int(os.environ.get("WORLD_SIZE", "1")) > 1
+                                     and not a.replicas):
+        run_sharded(a)
     else:
         run_ours(a)
 

@@ -204,6 +204,30 @@ class PeerExchange:
             self.handles = []
 
 
+def shard_primary_keys(pk, world, rank):
+    """Rank `rank`'s shard of a primary-key column spread over `world`
+    ranks: a permutation `pk` of 1..n becomes key = (pk - 1) * world + rank
+    + 1 (in place), so the shards of all ranks together are a permutation
+    of 1..world * n and no key is on two ranks."""
+    return pk.sub_(1).mul_(world).add_(rank + 1)
+
+
+class EngineJoin:
+    """Local join for exchange_join that keeps one RadixJoinEngine (sized for
+    at most max_build x max_probe tuples) across calls, instead of
+    allocating an engine per join."""
+
+    def __init__(self, max_build, max_probe, dtype, bits, scheme):
+        import fi_sqlops as fi
+        self.engine = fi.RadixJoinEngine(max(max_build, 1), max(max_probe, 1), dtype,
+                                         fi.RadixBits(*bits), scheme)
+
+    def __call__(self, rk, rp, sk, sp, bits, scheme):
+        s, c = self.engine.run(rk, rp, sk, sp)
+        self.engine.status()
+        return s, c
+
+
 def gpu_local_join(rk, rp, sk, sp, bits, scheme):
     import fi_sqlops as fi
     e = fi.RadixJoinEngine(max(rk.numel(), 1), max(sk.numel(), 1), rk.dtype,
@@ -215,12 +239,14 @@ def gpu_local_join(rk, rp, sk, sp, bits, scheme):
 
 def exchange_join(rk, rp, sk, sp, bits=(9, 9), scheme=None, group=None,
                   group_by=gpu_group_by_destination, local_join=gpu_local_join,
-                  exchange="nccl", peers=None):
+                  exchange="peer", peers=None):
     """Join of R and S sharded over the ranks: exchange on the bits above
     the local join's, join locally, add up.  Returns (sum, count) of the
-    whole join on every rank.  exchange="peer" uses the fused kernel through
-    `peers` = (PeerExchange for R, PeerExchange for S), created here (and
-    closed again) when not given."""
+    whole join on every rank.  exchange="peer" (the default) uses the fused
+    kernel through `peers` = (PeerExchange for R, PeerExchange for S),
+    created here (and closed again) when not given; exchange="nccl" groups
+    with `group_by` and moves the tuples with NCCL's all-to-all (also the
+    path for CPU tensors under gloo)."""
     if scheme is None:
         import fi_sqlops as fi
         scheme = fi.HashingScheme.BucketChaining

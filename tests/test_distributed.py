@@ -68,7 +68,8 @@ def worker(rank, world, port, dt, out):
         rk2, _ = D.shuffle(r, rp, sum(bits), group_by=cpu_group_by)
         assert bool((D.destinations(rk2, sum(bits), g) == rank).all())
         res = D.exchange_join(r, rp, s, sp, bits=bits, scheme=2,
-                              group_by=cpu_group_by, local_join=cpu_join)
+                              group_by=cpu_group_by, local_join=cpu_join,
+                              exchange="nccl")
         out.put((rank, res, rk2.numel()))
     finally:
         dist.destroy_process_group()
@@ -227,3 +228,44 @@ def test_peer_exchange_protocol_two_ranks():
             assert (b, c) == (base[d], 8000)
             if d != r:  # the peer's columns: mapped base + its offset, payloads after keys
                 assert kp == (1 << (20 + d)) + 16 * d and pp == kp + 8000 * 8
+
+
+def sharded_worker(rank, world, port, n, out):
+    """The sharded bench workload's host logic on gloo ranks: shards made by
+    the bench's rule (distributed.shard_primary_keys for R, a seed per rank
+    for S's uniform foreign keys over all ranks' keys, payload = key), the
+    exchange join, and its closed form."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        import distributed as D
+        import oracle as O
+        rk = torch.from_numpy(O.primary_keys(n, 7, np.int64))
+        D.shard_primary_keys(rk, world, rank)
+        sk = torch.from_numpy(O.uniform_foreign_keys(n, world * n, 8 + rank, np.int64))
+        part = torch.tensor([int(sk.sum())], dtype=torch.int64)
+        dist.all_reduce(part)
+        res = D.exchange_join(rk, rk.clone(), sk, sk.clone(), bits=(3, 3), scheme=2,
+                              group_by=cpu_group_by, local_join=cpu_join,
+                              exchange="nccl")
+        out.put((rank, res, int(part.item()), sorted(rk.tolist())))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_sharded_bench_rule(world):
+    """Every S key is a foreign key of the ranks' R shards, which together
+    are a permutation of 1..world*n: count = world * n, sum = all S keys."""
+    n = 1 << 12
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    mp.spawn(sharded_worker, args=(world, free_port(), n, out), nprocs=world, join=True)
+    got = sorted(out.get(timeout=60) for _ in range(world))
+    keys = sorted(k for g in got for k in g[3])
+    assert keys == list(range(1, world * n + 1))
+    for rank, (s, c), total, _ in got:
+        assert c == world * n
+        assert s == (total + (1 << 63)) % (1 << 64) - (1 << 63)

@@ -48,7 +48,8 @@ def test_exchange_join_one_rank_nccl(fi, oracle):
         n = 1 << 20
         r = oracle.primary_keys(n, 41, np.int64)
         s = oracle.uniform_foreign_keys(2 * n, 2 * n, 42, np.int64)
-        got = D.exchange_join(to_dev(r), to_dev(r), to_dev(s), to_dev(s), bits=(6, 6))
+        got = D.exchange_join(to_dev(r), to_dev(r), to_dev(s), to_dev(s), bits=(6, 6),
+                              exchange="nccl")
     finally:
         dist.destroy_process_group()
     exp_s, exp_c, _, _ = oracle.cpu_radix_join(r, r.copy(), s, s.copy(), 6, 6, 4,
