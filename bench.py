@@ -646,6 +646,18 @@ def run_sharded(a):
               else fi.HashingScheme.BucketChaining)
     stream = torch.cuda.current_stream()
     emulate = a.emulate_ranks if world == 1 else 1
+    own_group = False
+    if world == 1 and emulate == 1:
+        # one rank: the exchange's collectives still need a process group
+        import datetime
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port,
+                                rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=600))
+        own_group = True
     W = max(world, emulate)
     shift = sum(bits)
     g = D.exchange_bits(W)
@@ -791,7 +803,7 @@ def run_sharded(a):
                 "nvlink": nvlink, "e2e": e2e, "clocks": clocks,
                 "verified": bool(verified)}
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if world > 1 or own_group:
         dist.barrier()
         dist.destroy_process_group()
 
