@@ -102,13 +102,15 @@ def parse():
                     help="out-of-core join: |R| = |S| = 2^ooc_log2n int64 tuples")
     ap.add_argument("--ooc-block", type=int, default=0,
                     help="out-of-core join: tuples per streamed block (0 = default)")
-    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-requests", type=int, default=10000)
     ap.add_argument("--serve-max-build", type=int, default=1 << 28,
                     help="largest |R| of the served stream (log-uniform from 64K)")
     ap.add_argument("--serve-load", type=float, default=0.8,
                     help="arrival rate relative to the plain path's measured "
                          "capacity")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-repeats", type=int, default=1,
+                    help="serve workload: runs of each arm on the same stream")
     ap.add_argument("--serve-workers", type=int, default=1,
                     help="engines of the server that run large joins at once")
     ap.add_argument("--sweep", default="6,8,10,12,14,16,18",
@@ -1121,11 +1123,12 @@ def pctl(xs, q):
     return float(np.percentile(np.asarray(xs), q))
 
 
-def run_plain_calls(fi, torch, reqs, max_build, slice_):
+def run_plain_calls(fi, torch, reqs, max_build, slice_, t_start=None):
     """Back-to-back plain calls: one request after the other on one reused
     engine per tuple type (build once, probe slices), generating its
     relations with the same kernels.  Returns per-request (result, service
-    seconds)."""
+    seconds, completion time).  With t_start, request i starts no earlier
+    than t_start + its arrival (a live run of the arrival stream)."""
     engines = {tb: fi.RadixJoinEngine(max_build, slice_,
                                       torch.int64 if tb == 16 else torch.int32,
                                       fi.RadixBits(12, 10),
@@ -1135,6 +1138,10 @@ def run_plain_calls(fi, torch, reqs, max_build, slice_):
     for r in reqs:
         dt = torch.int64 if r["tb"] == 16 else torch.int32
         torch.cuda.synchronize()
+        if t_start is not None:
+            delay = t_start + r["arrival"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
         t0 = time.perf_counter()
         rk = torch.empty(r["rn"], dtype=dt, device="cuda")
         sk = torch.empty(r["sn"], dtype=dt, device="cuda")
@@ -1152,7 +1159,8 @@ def run_plain_calls(fi, torch, reqs, max_build, slice_):
         for o in range(0, r["sn"], slice_):
             s, c = e.probe(sk[o:o + slice_], sk[o:o + slice_])
             s_tot, c_tot = (s_tot + s) & ((1 << 64) - 1), c_tot + c
-        out.append(((s_tot, c_tot), time.perf_counter() - t0))
+        t1 = time.perf_counter()
+        out.append(((s_tot, c_tot), t1 - t0, t1))
         del rk, sk
     e = None
     engines.clear()
@@ -1161,11 +1169,13 @@ def run_plain_calls(fi, torch, reqs, max_build, slice_):
 
 def run_serve(a):
     """Served and batched joins against back-to-back plain calls on the same
-    request stream.  Plain: requests one after the other in arrival order
-    (start = max(arrival, previous finish)); served: a submitter thread
-    hands each request to the join server at its arrival time, the server
-    admits, batches and overlaps them.  Latency = completion - arrival;
-    throughput = all tuples / (last completion - first arrival)."""
+    request stream, both live: a first plain pass measures the service times
+    (the arrival rate is set from that capacity); then, --serve-repeats
+    times each, the plain arm runs the requests one after the other in
+    arrival order, each starting no earlier than its arrival, and the served
+    arm hands each request to the join server at its arrival time from a
+    submitter thread.  Latency = completion - arrival; throughput = all
+    tuples / (last completion - first arrival)."""
     import threading
     import torch
     import fi_sqlops as fi
@@ -1173,41 +1183,52 @@ def run_serve(a):
     reqs = serve_requests(a)
     slice_ = a.serve_max_build
     tuples = sum(r["rn"] + r["sn"] for r in reqs)
+    mask = (1 << 64) - 1
     # warm-up of both paths on a few requests (untimed)
     warm = reqs[:max(a.warmup, 1)]
+    for r in warm:
+        r["arrival"] = 0.0
     run_plain_calls(fi, torch, warm, a.serve_max_build, slice_)
     torch.cuda.empty_cache()
-    # plain: measured service times, then the arrival timeline at a fraction
-    # of the plain path's capacity
-    plain = run_plain_calls(fi, torch, reqs, a.serve_max_build, slice_)
+    # capacity from measured service times, then the arrival timeline
+    first = run_plain_calls(fi, torch, reqs, a.serve_max_build, slice_)
     torch.cuda.empty_cache()
-    rate = serve_arrivals(a, reqs, sum(p[1] for p in plain))
-    finish, plain_lat = 0.0, []
-    for r, (_, svc) in zip(reqs, plain):
-        finish = max(r["arrival"], finish) + svc
-        plain_lat.append(finish - r["arrival"])
-    plain_span = finish - reqs[0]["arrival"]
-    # served
-    srv = fi.JoinServer(hbm_budget_bytes=int(a.serve_budget_gb * 1e9),
-                        workers=a.serve_workers, max_build=a.serve_max_build,
-                        probe_slice=slice_)
-    for t in [srv.submit(tuple_bytes=r["tb"], build_len=r["rn"], probe_len=r["sn"],
-                         seed=r["seed"], zipf_s=r["zipf"]) for r in warm]:
-        srv.wait(t)
-    tickets = [None] * len(reqs)
-    lag = [0.0] * len(reqs)
+    rate = serve_arrivals(a, reqs, sum(p[1] for p in first))
+    expected = [p[0] for p in first]
+    verified = all(c == r["sn"] for (_, c), r in zip(expected, reqs))
 
-    def submitter(t_start):
-        for i, r in enumerate(reqs):
-            delay = t_start + r["arrival"] - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            lag[i] = time.perf_counter() - (t_start + r["arrival"])
-            tickets[i] = srv.submit(tuple_bytes=r["tb"], build_len=r["rn"],
-                                    probe_len=r["sn"], seed=r["seed"],
-                                    zipf_s=r["zipf"])
+    def plain_arm():
+        t_start = time.perf_counter() + 0.05
+        res = run_plain_calls(fi, torch, reqs, a.serve_max_build, slice_, t_start)
+        torch.cuda.empty_cache()
+        lat = [p[2] - (t_start + r["arrival"]) for p, r in zip(res, reqs)]
+        span = res[-1][2] - (t_start + reqs[0]["arrival"])
+        ok = all(p[0] == e for p, e in zip(res, expected))
+        return {"g_tuples_per_s": tuples / span / 1e9, "makespan_s": span,
+                "busy_g_tuples_per_s": tuples / sum(p[1] for p in res) / 1e9,
+                "p50_ms": 1e3 * pctl(lat, 50), "p99_ms": 1e3 * pctl(lat, 99),
+                "p999_ms": 1e3 * pctl(lat, 99.9)}, lat, ok
 
-    with ClockSampler(local) as clk:
+    def served_arm():
+        srv = fi.JoinServer(hbm_budget_bytes=int(a.serve_budget_gb * 1e9),
+                            workers=a.serve_workers, max_build=a.serve_max_build,
+                            probe_slice=slice_)
+        for t in [srv.submit(tuple_bytes=r["tb"], build_len=r["rn"], probe_len=r["sn"],
+                             seed=r["seed"], zipf_s=r["zipf"]) for r in warm]:
+            srv.wait(t)
+        tickets = [None] * len(reqs)
+        lag = [0.0] * len(reqs)
+
+        def submitter(t_start):
+            for i, r in enumerate(reqs):
+                delay = t_start + r["arrival"] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                lag[i] = time.perf_counter() - (t_start + r["arrival"])
+                tickets[i] = srv.submit(tuple_bytes=r["tb"], build_len=r["rn"],
+                                        probe_len=r["sn"], seed=r["seed"],
+                                        zipf_s=r["zipf"])
+
         t_start = time.perf_counter() + 0.05
         th = threading.Thread(target=submitter, args=(t_start,))
         th.start()
@@ -1218,18 +1239,46 @@ def run_serve(a):
             resp.append(srv.wait(tickets[i]))
         t_end = time.perf_counter()
         th.join()
+        stats = srv.stats()
+        srv.close()
+        lat = [g["latency_us"] / 1e6 + lag[i] for i, g in enumerate(resp)]
+        span = t_end - (t_start + reqs[0]["arrival"])
+        ok = all(g["status"] == 0 and ((g["sum"] & mask), g["count"]) == e
+                 for g, e in zip(resp, expected))
+        small = [i for i, g in enumerate(resp) if g["batched"]]
+        out = {"g_tuples_per_s": tuples / span / 1e9, "makespan_s": span,
+               "p50_ms": 1e3 * pctl(lat, 50), "p99_ms": 1e3 * pctl(lat, 99),
+               "p999_ms": 1e3 * pctl(lat, 99.9),
+               "small_p99_ms": 1e3 * pctl([lat[i] for i in small], 99) if small else None,
+               "batched_requests": len(small), "batches": stats["batches"],
+               "engine_runs": stats["engine_runs"],
+               "engine_busy_s": stats["engine_busy_us"] / 1e6,
+               "batch_busy_s": stats["batch_busy_us"] / 1e6,
+               "scheduler_enqueue_s": stats["enqueue_us"] / 1e6,
+               "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
+               "fixed_gb": stats["fixed_bytes"] / 1e9}
+        return out, small, ok
+
+    served_runs, plain_runs = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(max(a.serve_repeats, 1)):
+            sv, small, ok_s = served_arm()
+            pl, plat, ok_p = plain_arm()
+            pl["small_p99_ms"] = 1e3 * pctl([plat[i] for i in small], 99) if small else None
+            served_runs.append(sv)
+            plain_runs.append(pl)
+            verified = verified and ok_s and ok_p
     clocks = clk.summary()
-    stats = srv.stats()
-    srv.close()
-    served_lat = [g["latency_us"] / 1e6 + lag[i] for i, g in enumerate(resp)]
-    served_span = t_end - (t_start + reqs[0]["arrival"])
-    verified = all(g["status"] == 0 and (g["sum"] & ((1 << 64) - 1), g["count"]) ==
-                   p[0] and g["count"] == r["sn"]
-                   for g, p, r in zip(resp, plain, reqs))
-    small = [i for i, g in enumerate(resp) if g["batched"]]
+
+    def spread(runs, key):
+        xs = [r[key] for r in runs]
+        return {"mean": sum(xs) / len(xs), "min": min(xs), "max": max(xs)}
+
+    served, plain = served_runs[-1], plain_runs[-1]
     if rank == 0:
         line = {"metric": "served radix join G tuples/s",
-                "value": tuples / served_span / 1e9, "unit": "G tuples/s",
+                "value": spread(served_runs, "g_tuples_per_s")["mean"],
+                "unit": "G tuples/s",
                 "n_gpus": world, "steps": len(reqs), "warmup": len(warm),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "int32+int64",
@@ -1241,29 +1290,14 @@ def run_serve(a):
                            "arrival_rate_per_s": rate, "offered_load": a.serve_load,
                            "hbm_budget_gb": a.serve_budget_gb,
                            "server_workers": a.serve_workers,
+                           "repeats": len(served_runs),
                            "l2_flush": "none: relations of most requests exceed L2"},
-                "served": {"g_tuples_per_s": tuples / served_span / 1e9,
-                           "makespan_s": served_span,
-                           "p50_ms": 1e3 * pctl(served_lat, 50),
-                           "p99_ms": 1e3 * pctl(served_lat, 99),
-                           "p999_ms": 1e3 * pctl(served_lat, 99.9),
-                           "small_p99_ms": 1e3 * pctl([served_lat[i] for i in small], 99)
-                           if small else None,
-                           "batched_requests": len(small), "batches": stats["batches"],
-                           "engine_runs": stats["engine_runs"],
-                           "engine_busy_s": stats["engine_busy_us"] / 1e6,
-                           "batch_busy_s": stats["batch_busy_us"] / 1e6,
-                           "scheduler_enqueue_s": stats["enqueue_us"] / 1e6,
-                           "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
-                           "fixed_gb": stats["fixed_bytes"] / 1e9},
-                "plain": {"g_tuples_per_s": tuples / plain_span / 1e9,
-                          "makespan_s": plain_span,
-                          "busy_g_tuples_per_s": tuples / sum(p[1] for p in plain) / 1e9,
-                          "p50_ms": 1e3 * pctl(plain_lat, 50),
-                          "p99_ms": 1e3 * pctl(plain_lat, 99),
-                          "p999_ms": 1e3 * pctl(plain_lat, 99.9),
-                          "small_p99_ms": 1e3 * pctl([plain_lat[i] for i in small], 99)
-                          if small else None},
+                "served": served, "plain": plain,
+                "repeats": {"served_g_tuples_per_s": spread(served_runs, "g_tuples_per_s"),
+                            "plain_g_tuples_per_s": spread(plain_runs, "g_tuples_per_s"),
+                            "served_p99_ms": spread(served_runs, "p99_ms"),
+                            "plain_p99_ms": spread(plain_runs, "p99_ms"),
+                            "served_runs": served_runs, "plain_runs": plain_runs},
                 "clocks": clocks, "verified": bool(verified)}
         print(json.dumps(line), flush=True)
     if world > 1:

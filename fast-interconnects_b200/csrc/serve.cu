@@ -25,8 +25,9 @@
 //  * large joins run on a worker: a resident engine on its own stream,
 //    planned by the autotuner, built once and probed in slices of
 //    probe_slice tuples.  A free worker takes the shortest admitted large
-//    join (or one that has waited over 0.5 s), and the next one is loaded on
-//    a load stream while the current one runs.  Workers overlap with each other and with batches (one worker by
+//    join (or one that has waited over 0.5 s); a worker keeps two joins
+//    enqueued on its stream, so the next starts without a host round trip,
+//    and the one after is loaded on a load stream while they run.  Workers overlap with each other and with batches (one worker by
 //    default: two large joins at once each run at half speed, which only
 //    lengthens their latency).
 //  * completion: the scheduler thread polls the done events, releases the
@@ -78,15 +79,29 @@ struct Request {
 
 constexpr uint32_t kMaxSlices = 64;
 
-struct Worker {
-  fi_radix_join_engine *engine = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t start = nullptr, done = nullptr;  // timing events
+// One large join enqueued on a worker: its timing events and result
+// buffers.
+struct Slot {
+  cudaEvent_t start = nullptr, done = nullptr;
   fi_join_result *d_res = nullptr;  // [kMaxSlices]
   fi_join_result *h_res = nullptr;  // pinned [kMaxSlices + 1]; the engine's
                                     // error word after the last slice
   uint32_t slices = 0;
   Request *req = nullptr;
+};
+
+// A worker keeps up to kWorkerSlots large joins enqueued on its stream: the
+// next one waits on the stream behind the running one (stream order keeps
+// the shared engine safe), so the GPU does not idle while the host notices
+// a completion and enqueues the next join.
+constexpr uint32_t kWorkerSlots = 2;
+
+struct Worker {
+  fi_radix_join_engine *engine = nullptr;
+  cudaStream_t stream = nullptr;
+  Slot slot[kWorkerSlots];
+  uint32_t head = 0;   // oldest enqueued slot
+  uint32_t count = 0;  // slots enqueued
 };
 
 // Host-side first-fit allocator over one device slab that holds the
@@ -365,14 +380,14 @@ bool fi_join_server::dispatch_batches(Clock::time_point now) {
   return progress;
 }
 
-static int run_large(Worker &w, Request *r, uint64_t slice) {
+static int run_large(Worker &w, Slot &sl, Request *r, uint64_t slice) {
   const fi_join_request &q = r->req;
   const fi_tuned_plan &p = r->plan;
   if (r->ready) {
     cudaError_t ce = cudaStreamWaitEvent(w.stream, r->ready, 0);
     if (ce != cudaSuccess) return cuda_error(ce, "stream wait");
   }
-  cudaEventRecord(w.start, w.stream);
+  cudaEventRecord(sl.start, w.stream);
   fi_join_plan jp{p.radix_bits, p.hashing_scheme, p.join_block, p.scatter};
   int rc = fi_radix_join_engine_set_plan(w.engine, &jp);
   if (rc) return rc;
@@ -380,37 +395,37 @@ static int run_large(Worker &w, Request *r, uint64_t slice) {
   if (sn > slice * kMaxSlices)
     return set_error(FI_ERR_CAPACITY, "probe relation needs more than %u slices",
                      kMaxSlices);
-  w.slices = sn ? (uint32_t)((sn + slice - 1) / slice) : 0;
+  sl.slices = sn ? (uint32_t)((sn + slice - 1) / slice) : 0;
   fi_stream_t st = (fi_stream_t)w.stream;
   if (q.tuple_bytes == 16) {
     rc = fi_radix_join_engine_build_int64(w.engine, (const int64_t *)r->cols[0],
                                           (const int64_t *)r->cols[1], q.build_len, st);
-    for (uint32_t s = 0; !rc && s < w.slices; ++s) {
+    for (uint32_t s = 0; !rc && s < sl.slices; ++s) {
       const uint64_t o = (uint64_t)s * slice, n = std::min(slice, sn - o);
       rc = fi_radix_join_engine_probe_int64(
           w.engine, (const int64_t *)r->cols[2] + o, (const int64_t *)r->cols[3] + o,
-          n, w.d_res + s, st);
+          n, sl.d_res + s, st);
     }
   } else {
     rc = fi_radix_join_engine_build_int32(w.engine, (const int32_t *)r->cols[0],
                                           (const int32_t *)r->cols[1], q.build_len, st);
-    for (uint32_t s = 0; !rc && s < w.slices; ++s) {
+    for (uint32_t s = 0; !rc && s < sl.slices; ++s) {
       const uint64_t o = (uint64_t)s * slice, n = std::min(slice, sn - o);
       rc = fi_radix_join_engine_probe_int32(
           w.engine, (const int32_t *)r->cols[2] + o, (const int32_t *)r->cols[3] + o,
-          n, w.d_res + s, st);
+          n, sl.d_res + s, st);
     }
   }
   if (rc) return rc;
-  if (w.slices) {
-    cudaError_t ce = cudaMemcpyAsync(w.h_res, w.d_res, w.slices * sizeof(fi_join_result),
+  if (sl.slices) {
+    cudaError_t ce = cudaMemcpyAsync(sl.h_res, sl.d_res, sl.slices * sizeof(fi_join_result),
                                      cudaMemcpyDeviceToHost, w.stream);
     if (ce != cudaSuccess) return cuda_error(ce, "result copy");
   }
   // the engine's error word, without a device-wide synchronisation
-  rc = fi_radix_join_engine_status_async(w.engine, (int *)(w.h_res + kMaxSlices), st);
+  rc = fi_radix_join_engine_status_async(w.engine, (int *)(sl.h_res + kMaxSlices), st);
   if (rc) return rc;
-  cudaError_t ce = cudaEventRecord(w.done, w.stream);
+  cudaError_t ce = cudaEventRecord(sl.done, w.stream);
   if (ce != cudaSuccess) return cuda_error(ce, "event record");
   return FI_OK;
 }
@@ -418,26 +433,29 @@ static int run_large(Worker &w, Request *r, uint64_t slice) {
 bool fi_join_server::dispatch_large() {
   bool progress = false;
   for (Worker &w : workers) {
-    if (w.req || large_q.empty()) continue;
-    auto pick = next_large(Clock::now());
-    Request *r = *pick;
-    large_q.erase(pick);
-    progress = true;
-    if (r->req.build_len > cfg.max_build) {
-      finish(r, set_error(FI_ERR_CAPACITY,
-                          "build relation above the server's max_build"));
-      continue;
-    }
-    if (!r->loaded) load(r, w.stream);
-    const int rc = fatal ? fatal : run_large(w, r, cfg.probe_slice);
-    if (rc) {
-      // the engine may hold work of this request: wait for it before the
-      // relations are released
-      cudaStreamSynchronize(w.stream);
-      finish(r, rc);
-    } else {
-      w.req = r;
-      ++stats.engine_runs;
+    while (w.count < kWorkerSlots && !large_q.empty() && !fatal) {
+      auto pick = next_large(Clock::now());
+      Request *r = *pick;
+      large_q.erase(pick);
+      progress = true;
+      if (r->req.build_len > cfg.max_build) {
+        finish(r, set_error(FI_ERR_CAPACITY,
+                            "build relation above the server's max_build"));
+        continue;
+      }
+      Slot &sl = w.slot[(w.head + w.count) % kWorkerSlots];
+      if (!r->loaded) load(r, w.stream);
+      const int rc = run_large(w, sl, r, cfg.probe_slice);
+      if (rc) {
+        // the engine may hold work of this request: wait for it before the
+        // relations are released
+        cudaStreamSynchronize(w.stream);
+        finish(r, rc);
+      } else {
+        sl.req = r;
+        ++w.count;
+        ++stats.engine_runs;
+      }
     }
   }
   // prefetch: load the next large join while the workers run, so that its
@@ -472,31 +490,37 @@ std::deque<Request *>::iterator fi_join_server::next_large(Clock::time_point now
 bool fi_join_server::complete() {
   bool progress = false;
   for (Worker &w : workers) {
-    if (!w.req) continue;
-    const cudaError_t ce = cudaEventQuery(w.done);
-    if (ce == cudaErrorNotReady) continue;
-    Request *r = w.req;
-    w.req = nullptr;
-    progress = true;
-    if (ce != cudaSuccess) {
-      fatal = cuda_error(ce, "large join");
-      finish(r, fatal);
-      continue;
+    // a worker's joins finish in the order they were enqueued
+    while (w.count > 0) {
+      Slot &sl = w.slot[w.head];
+      const cudaError_t ce = cudaEventQuery(sl.done);
+      if (ce == cudaErrorNotReady) break;
+      Request *r = sl.req;
+      sl.req = nullptr;
+      w.head = (w.head + 1) % kWorkerSlots;
+      --w.count;
+      progress = true;
+      if (ce != cudaSuccess) {
+        fatal = cuda_error(ce, "large join");
+        finish(r, fatal);
+        continue;
+      }
+      uint64_t sum = 0, count = 0;
+      for (uint32_t s = 0; s < sl.slices; ++s) {
+        sum += (uint64_t)sl.h_res[s].sum;
+        count += sl.h_res[s].count;
+      }
+      r->resp.result.sum = (int64_t)sum;
+      r->resp.result.count = count;
+      const int dev = *(const int *)(sl.h_res + kMaxSlices);
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, sl.start, sl.done) == cudaSuccess)
+        stats.engine_busy_us += 1e3 * ms;
+      finish(r, dev == 0 ? FI_OK
+                         : set_error(dev == FI_ERR_TIMEOUT ? FI_ERR_TIMEOUT
+                                                           : FI_ERR_RUNTIME,
+                                     "device-side error %d in a large join", dev));
     }
-    uint64_t sum = 0, count = 0;
-    for (uint32_t s = 0; s < w.slices; ++s) {
-      sum += (uint64_t)w.h_res[s].sum;
-      count += w.h_res[s].count;
-    }
-    r->resp.result.sum = (int64_t)sum;
-    r->resp.result.count = count;
-    const int dev = *(const int *)(w.h_res + kMaxSlices);
-    float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, w.start, w.done) == cudaSuccess)
-      stats.engine_busy_us += 1e3 * ms;
-    finish(r, dev == 0 ? FI_OK
-                       : set_error(dev == FI_ERR_TIMEOUT ? FI_ERR_TIMEOUT : FI_ERR_RUNTIME,
-                                   "device-side error %d in a large join", dev));
   }
   for (Runner &run : runners) {
     if (!run.batch.busy()) continue;
@@ -550,7 +574,7 @@ void fi_join_server::loop() {
         }
     }
     bool busy = false;
-    for (Worker &w : workers) busy |= w.req != nullptr;
+    for (Worker &w : workers) busy |= w.count > 0;
     for (Runner &r : runners) busy |= r.batch.busy();
     const bool queued = !pending.empty() || !small_q[0].empty() ||
                         !small_q[1].empty() || !large_q.empty();
@@ -570,10 +594,12 @@ void fi_join_server::teardown() {
   for (Worker &w : workers) {
     if (w.stream) cudaStreamSynchronize(w.stream);
     if (w.engine) fi_radix_join_engine_free(w.engine);
-    if (w.d_res) cudaFree(w.d_res);
-    if (w.h_res) cudaFreeHost(w.h_res);
-    if (w.done) cudaEventDestroy(w.done);
-    if (w.start) cudaEventDestroy(w.start);
+    for (Slot &sl : w.slot) {
+      if (sl.d_res) cudaFree(sl.d_res);
+      if (sl.h_res) cudaFreeHost(sl.h_res);
+      if (sl.done) cudaEventDestroy(sl.done);
+      if (sl.start) cudaEventDestroy(sl.start);
+    }
     if (w.stream) cudaStreamDestroy(w.stream);
   }
   workers.clear();
@@ -634,12 +660,17 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
                                   FI_HASHING_BUCKET_CHAINING, &w.engine);
     if (rc) break;
     s->fixed += fi_radix_join_engine_workspace_bytes(w.engine);
-    if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) ||
-        (ce = cudaEventCreate(&w.done)) || (ce = cudaEventCreate(&w.start)) ||
-        (ce = cudaMalloc((void **)&w.d_res, kMaxSlices * sizeof(fi_join_result))) ||
-        (ce = cudaHostAlloc((void **)&w.h_res, (kMaxSlices + 1) * sizeof(fi_join_result),
-                            cudaHostAllocDefault)))
+    if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) != cudaSuccess)
       rc = cuda_error(ce, "worker set-up");
+    for (Slot &sl : w.slot) {
+      if (rc) break;
+      if ((ce = cudaEventCreate(&sl.done)) || (ce = cudaEventCreate(&sl.start)) ||
+          (ce = cudaMalloc((void **)&sl.d_res, kMaxSlices * sizeof(fi_join_result))) ||
+          (ce = cudaHostAlloc((void **)&sl.h_res,
+                              (kMaxSlices + 1) * sizeof(fi_join_result),
+                              cudaHostAllocDefault)))
+        rc = cuda_error(ce, "worker set-up");
+    }
   }
   if (!rc) {
     s->runners = std::vector<Runner>(4);
