@@ -1527,6 +1527,14 @@ def run_nopart(a):
                              "peak": peak, "unit": "GB/s",
                              "frac": probe_bytes / (probe_ms / 1e3) / 1e9 / peak,
                              "peak_source": peak_kind, "traffic": None},
+                # the same probe against the DRAM-sector bound: each table
+                # access moves at least one 32-byte sector, plus the probe
+                # tuple streamed; and as random sectors per second
+                "sector_roofline": {
+                    "bytes_per_probe": 32 + 2 * tb,
+                    "achieved_gb_per_s": npr * (32 + 2 * tb) / (probe_ms / 1e3) / 1e9,
+                    "frac": npr * (32 + 2 * tb) / (probe_ms / 1e3) / 1e9 / peak,
+                    "probes_per_s": npr / (probe_ms / 1e3)},
                 "cpu_baseline": cpu,
                 "clocks": clk.summary(), "verified": bool(verified)}
         print(json.dumps(line), flush=True)

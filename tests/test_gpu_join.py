@@ -180,6 +180,34 @@ def test_hash_join(fi, oracle, ndt, tdt, scheme):
     assert got == exp
 
 
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("size,n_b,n_p", [(1, 1, 50), (2, 2, 77), (3, 2, 64),
+                                          (4, 3, 500), (8, 7, 999), (64, 60, 5000),
+                                          (1024, 1000, 20011), (5000, 3000, 40009)])
+def test_hash_join_linear_probing_windows(fi, oracle, ndt, tdt, size, n_b, n_p):
+    """Linear probing loads a window of slots per step (4 int64 / 8 int32
+    entries, the int32 window from the hash slot's aligned pair): tables of
+    1..8 slots where a window wraps onto itself, nearly full tables whose
+    probes cross many windows, duplicate build keys and misses; the sums
+    equal the oracle's (pinned to the reference's compiled CPU join)."""
+    rng = np.random.default_rng(size * 7 + n_p)
+    lg = size.bit_length() - 1
+    slots = 1 << lg  # the reference hashes into 2^floor(log2(size)) slots
+    n_b = min(n_b, slots)  # every build tuple finds a slot
+    r_key = rng.integers(0, max(2, n_b // 2 + 1), n_b).astype(ndt)  # duplicates
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    s_key = rng.integers(0, n_b + 3, n_p).astype(ndt)  # some miss
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    ht = fi.HashTable(size, tdt)
+    hj = fi.CudaHashJoin(fi.HashingScheme.LinearProbing, ht, (37, 128), (37, 128))
+    hj.build(to_dev(r_key), to_dev(r_pay))
+    res = torch.zeros(37 * 128, dtype=torch.int64, device="cuda")
+    hj.probe_sum(to_dev(s_key), to_dev(s_pay), res)
+    got = int(to_host(res).astype(np.uint64).sum(dtype=np.uint64))
+    exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got == exp
+
+
 def test_hash_join_selective_perfect(fi, oracle):
     n = 50000
     r_key = oracle.primary_keys(n, 3, np.int64, base=0)
