@@ -145,3 +145,15 @@ def test_reference_gpu_harness_exports():
         assert hasattr(lib, name), name
     assert lib.rg_padding_len(C.c_int(4)) == 16
     assert lib.rg_padding_len(C.c_int(8)) == 8
+
+
+def test_cpp_host_api_builds():
+    """The C++ host API (include/fi_sqlops.hpp) and its test program compile
+    and link against the library (run on a GPU by test_gpu_host_api.py)."""
+    import subprocess
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run(["make", "-s", "-C", os.path.join(here, "cpp")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert os.path.exists(os.path.join(here, "cpp", "_build", "host_api_test"))
