@@ -11,7 +11,8 @@
 //    calls no CUDA allocator and frees nothing that the GPU still reads.
 //  * admission: a request is admitted when its relations (when the server
 //    holds them) get a block of the slab.  Requests are admitted in arrival
-//    order; one larger than the whole slab fails with FI_ERR_CAPACITY.
+//    order, except that small joins may pass a large one that waits for
+//    memory; one larger than the whole slab fails with FI_ERR_CAPACITY.
 //  * loading: server-held relations (host or synthetic sources) are copied
 //    or generated: those of small joins at admission on a high-priority load
 //    stream (an event marks them ready), those of large joins on their
@@ -554,10 +555,29 @@ void fi_join_server::loop() {
   for (;;) {
     bool progress = false;
     const Clock::time_point t0 = Clock::now();
-    while (!pending.empty() && !fatal) {
-      if (!admit(pending.front())) break;
-      pending.pop_front();
-      progress = true;
+    // Admission in arrival order.  When the oldest request waits for arena
+    // memory, the small joins among the next kAdmitWindow requests (a few MB
+    // each) may still take a block, so that they do not wait behind a large
+    // one; large requests keep their order, so none is passed over for good.
+    constexpr size_t kAdmitWindow = 64;
+    bool blocked = false;
+    size_t looked = 0;
+    for (auto it = pending.begin(); it != pending.end() && !fatal;) {
+      Request *r = *it;
+      if (blocked) {
+        if (++looked > kAdmitWindow) break;
+        if (r->req.build_len + r->req.probe_len > cfg.small_tuples) {
+          ++it;
+          continue;
+        }
+      }
+      if (admit(r)) {
+        it = pending.erase(it);
+        progress = true;
+      } else {
+        blocked = true;
+        ++it;
+      }
     }
     progress |= complete();
     if (!fatal) {
