@@ -306,14 +306,16 @@ static uint32_t log2_floor_u64(uint64_t x) {
                                                                                \
   /* No-partitioning linear-probing build,                                     \
    * sql-ops/cpputils/no_partitioning_join.cpp:27-86: slot = hash(key) mod     \
-   * 2^log2(entries), probe forward until a null key. */                      \
+   * 2^log2(entries), probe forward until a null key.  A one-slot table       \
+   * (log2 = 0) hashes to slot 0: the reference shifts by the full word width \
+   * there, which is undefined. */                                            \
   void or_ht_build_linearprobing_##SUF(or_tuple_##SUF *ht, uint64_t entries,   \
                                        const K *keys, const K *pays,           \
                                        uint64_t len) {                         \
     uint32_t lg = log2_floor_u64(entries);                                     \
     uint64_t n = 1ull << lg, m = n - 1;                                        \
     for (uint64_t t = 0; t < len; ++t) {                                       \
-      uint64_t idx = (uint64_t)HASHFN((uint64_t)(int64_t)keys[t], lg);         \
+      uint64_t idx = lg ? (uint64_t)HASHFN((uint64_t)(int64_t)keys[t], lg) : 0;\
       for (uint64_t i = 0; i < n; ++i, idx = (idx + 1) & m) {                  \
         if (ht[idx].key == (K)-1) {                                            \
           ht[idx].key = keys[t];                                               \
@@ -333,7 +335,7 @@ static uint32_t log2_floor_u64(uint64_t x) {
     uint32_t lg = log2_floor_u64(entries);                                     \
     uint64_t n = 1ull << lg, m = n - 1, sum = 0;                               \
     for (uint64_t t = 0; t < len; ++t) {                                       \
-      uint64_t idx = (uint64_t)HASHFN((uint64_t)(int64_t)keys[t], lg);         \
+      uint64_t idx = lg ? (uint64_t)HASHFN((uint64_t)(int64_t)keys[t], lg) : 0;\
       for (uint64_t i = 0; i < n; ++i, idx = (idx + 1) & m) {                  \
         if (ht[idx].key == keys[t])                                            \
           sum += (uint64_t)(int64_t)pays[t];                                   \

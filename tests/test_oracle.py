@@ -216,3 +216,18 @@ def test_oracle_radix_join_matches_compiled_reference(oracle, kind, name, dt):
             s, c, _, _ = oracle.cpu_radix_join(rk, rp, sk, sp, 4, 5, 4,
                                                use_reference=use_ref)
             assert (np.uint64(s % (1 << 64)), c) == (np.uint64(exp_s), exp_c), use_ref
+
+
+@pytest.mark.parametrize("dt", [np.int32, np.int64])
+def test_oracle_linear_probing_tiny_tables(oracle, dt):
+    """Tables of 1..8 slots (one slot: the reference's hash would shift by
+    the whole word width, undefined; slot 0 here, as on the GPU): every
+    probe key adds its payload once per equal build key."""
+    for size in (1, 2, 3, 4, 8):
+        slots = 1 << (size.bit_length() - 1)
+        r = np.array([0, 0, 1, 5, 7, 0, 3, 1][:slots], dt)
+        s = np.array([0, 1, 2, 0, 7, 9], dt)
+        sp = np.array([1, 2, 3, 4, 5, 6], dt)
+        got, _ = oracle.ht_linearprobing_sum(r, r + 5, s, sp, size)
+        exp = sum(int(p) * int((r == k).sum()) for k, p in zip(s, sp))
+        assert got == exp, size
