@@ -17,8 +17,11 @@
 // probing builds in 1.0 ms and probes in 11.1 ms (a 2^25-entry, 512 MB
 // table: one random access per probe, far beyond the 126 MB L2), perfect
 // hashing probes in 4.7 ms (16M + 1 entries).  Four tuples per thread with
-// their table loads issued together made it no faster (11.7 ms): the probe
-// is bound by random HBM accesses, not by their latency.  The table size
+// their table loads issued together made it no faster (11.7 ms), nor did
+// loading a window of 4 slots (64 B) per step instead of slot by slot (11.0
+// ms): the probe is bound by the rate of random HBM accesses (about 30 G/s
+// reach DRAM in both schemes), and the perfect table is faster because it is
+// half the size, so twice as much of it stays in L2.  The table size
 // matters more: the hash masks with 2^floor(log2(size)) (as the reference
 // does), so a size that is not a power of two can fill the table to near
 // 1 (Kim, 128e6 keys in 2^27 slots: 27 ms per probe against 5.8 ms in 2^28).
@@ -96,61 +99,11 @@ __global__ void ht_build_perfect_kernel(Tuple<K> *ht, uint64_t size,
   }
 }
 
-// Probe window: the slots a probe loads at once, as independent vector
-// loads, before it looks at any of them.  int64 entries: 4 slots of 16 B
-// from the hash slot on; int32 entries: the 8 slots of the 16-byte-aligned
-// pairs from the hash slot's pair on (the first may precede the hash slot
-// and is skipped).  Loading the window together lets the second sector of a
-// probe ride the DRAM row the first one opened: probing slot by slot, each
-// dependent load arrived after the row had closed (Blanas, 16M x 256M int64
-// in 2^25 slots: 11.1 ms per probe slot by slot).
-template <typename K>
-struct ProbeWindow;
-template <>
-struct ProbeWindow<int64_t> {
-  static constexpr uint32_t kSlots = 4;
-  __device__ __forceinline__ static uint64_t first(uint64_t idx) { return idx; }
-};
-template <>
-struct ProbeWindow<int32_t> {
-  static constexpr uint32_t kSlots = 8;
-  __device__ __forceinline__ static uint64_t first(uint64_t idx) { return idx & ~1ull; }
-};
-
-__device__ __forceinline__ void load_window(const Tuple<int64_t> *ht, uint64_t base,
-                                            uint64_t m, int64_t (&keys)[4]) {
-  longlong2 e[4];
-#pragma unroll
-  for (uint32_t j = 0; j < 4; ++j)
-    e[j] = *reinterpret_cast<const longlong2 *>(ht + ((base + j) & m));
-#pragma unroll
-  for (uint32_t j = 0; j < 4; ++j) keys[j] = e[j].x;
-}
-__device__ __forceinline__ void load_window(const Tuple<int32_t> *ht, uint64_t base,
-                                            uint64_t m, int32_t (&keys)[8]) {
-  // a table of one slot has no pair: load it alone
-  if (m == 0) {
-#pragma unroll
-    for (uint32_t j = 0; j < 8; ++j) keys[j] = ht[0].key;
-    return;
-  }
-  int4 e[4];
-#pragma unroll
-  for (uint32_t j = 0; j < 4; ++j)
-    e[j] = *reinterpret_cast<const int4 *>(ht + ((base + 2 * j) & m));
-#pragma unroll
-  for (uint32_t j = 0; j < 4; ++j) {
-    keys[2 * j] = e[j].x;
-    keys[2 * j + 1] = e[j].z;
-  }
-}
-
 template <typename K>
 __global__ void ht_probe_lp_kernel(const Tuple<K> *__restrict__ ht,
                                    uint64_t size, const K *__restrict__ key,
                                    const K *__restrict__ pay, uint64_t len,
                                    uint64_t *__restrict__ result) {
-  using W = ProbeWindow<K>;
   const uint32_t lg = log2_floor_u64(size);
   const uint64_t n = 1ull << lg, m = n - 1;
   const uint64_t gid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -158,27 +111,13 @@ __global__ void ht_probe_lp_kernel(const Tuple<K> *__restrict__ ht,
   for (uint64_t i = gid; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
     const K k = load_cs(key + i);
     const K v = load_cs(pay + i);
-    const uint64_t h = lg ? mult_shift_hash<K>(k, lg) : 0;
-    // slots h, h+1, ... (mod n) in order until an empty one, each slot
-    // once: at most n slots, as the reference's probe loop
-    uint64_t base = W::first(h);
-    uint32_t skip = (uint32_t)(h - base);
-    uint64_t seen = 0;
-    bool open = true;
-    while (open && seen < n) {
-      K w[W::kSlots];
-      load_window(ht, base, m, w);
-#pragma unroll
-      for (uint32_t j = 0; j < W::kSlots; ++j) {
-        if (!open || j < skip || seen >= n) continue;
-        ++seen;
-        if (w[j] == k)
-          sum += static_cast<uint64_t>(static_cast<int64_t>(v));
-        else if (w[j] == null_key<K>())
-          open = false;
-      }
-      skip = 0;
-      base = (base + W::kSlots) & m;
+    uint64_t idx = lg ? mult_shift_hash<K>(k, lg) : 0;
+    for (uint64_t s = 0; s < n; ++s, idx = (idx + 1) & m) {
+      const Tuple<K> e = load_tuple(ht + idx);
+      if (e.key == k)
+        sum += static_cast<uint64_t>(static_cast<int64_t>(v));
+      else if (e.key == null_key<K>())
+        break;
     }
   }
   result[gid] += sum;
