@@ -140,7 +140,8 @@ def load_peaks():
 
 def load_traffic():
     """DRAM traffic per launch of the dominant kernels from the committed ncu
-    summary (profiles/traffic.json), if present."""
+    summary (profiles/traffic.json: measured on a 64M x 64M case and scaled
+    to a 1024M x 1024M launch), if present."""
     path = os.path.join(REPO, "profiles", "traffic.json")
     try:
         with open(path) as f:
@@ -420,6 +421,8 @@ def run_ours(a):
                 "peak": peak, "unit": "GB/s", "frac": d["gb_per_s"] / peak,
                 "peak_source": peak_kind,
                 "traffic": traffic,
+                "traffic_source": "ncu dram bytes per launch of a 64M x 64M capture, "
+                                  "scaled x16 (profiles/traffic.json)",
                 "launch_ms": d["ms"] / 2 if dominant != "join" else d["ms"],
                 "algorithmic_bytes_per_launch":
                     d["algorithmic_bytes"] // (1 if dominant == "join" else 2)}
