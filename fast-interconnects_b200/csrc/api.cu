@@ -808,7 +808,34 @@ struct fi_cuda_hash_join {
   void *ht;
   uint64_t mem_len, size;
   uint32_t bg, bb, pg, pb;
+  // region-ordered probing: on by default, slices of probe_slice tuples
+  bool grouping = true;
+  uint64_t probe_slice = 1ull << 27;
+  DevBuf group_tuples, group_counts;
 };
+
+// Probe sides of at least one probe per table slot, on tables larger than a
+// region (8 MB), are grouped by table region before probing.
+static bool use_grouping(const fi_cuda_hash_join *h, uint64_t len, uint32_t entry_bytes,
+                         uint32_t *region_bits) {
+  if (!h->grouping) return false;
+  *region_bits = ht_region_bits(h->size, entry_bytes);
+  const uint64_t slots = 1ull << (63 - __builtin_clzll(h->size));
+  return *region_bits > 0 && len >= slots;
+}
+
+extern "C" int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj,
+                                                    int enable,
+                                                    uint64_t slice_tuples) {
+  if (!hj) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  if (enable && slice_tuples == 0)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "slice_tuples must be at least 1");
+  if (slice_tuples >= 0xffffffffull)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "slice_tuples must be below 2^32");
+  hj->grouping = enable != 0;
+  if (enable) hj->probe_slice = slice_tuples;
+  return FI_OK;
+}
 
 extern "C" int fi_hash_table_init_int32(void *ht_mem, uint64_t mem_len,
                                         fi_stream_t stream) {
@@ -849,7 +876,12 @@ extern "C" int fi_cuda_hash_join_new(fi_hashing_scheme hashing_scheme,
   return FI_OK;
 }
 
-extern "C" void fi_cuda_hash_join_free(fi_cuda_hash_join *hj) { delete hj; }
+extern "C" void fi_cuda_hash_join_free(fi_cuda_hash_join *hj) {
+  if (!hj) return;
+  hj->group_tuples.release();
+  hj->group_counts.release();
+  delete hj;
+}
 
 template <typename K>
 static int hj_build_impl(fi_cuda_hash_join *h, const K *key, const K *pay,
@@ -877,6 +909,18 @@ static int hj_probe_impl(fi_cuda_hash_join *h, const K *key, const K *pay,
                      "Result set size is too small, must be at least grid * block size");
   if (h->scheme == FI_HASHING_BUCKET_CHAINING)
     return set_error(FI_ERR_UNSUPPORTED, "hashing scheme not implemented");
+  uint32_t region_bits = 0;
+  if (len > 0 && use_grouping(h, len, 2 * sizeof(K), &region_bits)) {
+    const uint64_t slice = std::min(len, h->probe_slice);
+    int rc = h->group_tuples.reserve(slice * 2 * sizeof(K), false);
+    if (!rc) rc = h->group_counts.reserve(ht_region_scratch_bytes(region_bits), false);
+    if (rc) return rc;
+    cudaError_t e = launch_ht_probe_grouped<K>(
+        h->scheme == FI_HASHING_LINEAR_PROBING ? 1 : 0, h->ht, h->size, key, pay,
+        len, result, h->pg, h->pb, region_bits, h->group_tuples.ptr,
+        (uint32_t *)h->group_counts.ptr, slice, (uint32_t)device_sm_count(), stream);
+    return e == cudaSuccess ? FI_OK : cuda_error(e, "hash table probe");
+  }
   cudaError_t e = launch_ht_probe_sum<K>(
       h->scheme == FI_HASHING_LINEAR_PROBING ? 1 : 0, h->ht, h->size, key, pay,
       len, result, h->pg, h->pb, stream);

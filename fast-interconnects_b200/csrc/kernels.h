@@ -145,6 +145,20 @@ cudaError_t launch_ht_probe_sum(int scheme, const void *ht, uint64_t ht_size,
                                 uint64_t *result, uint32_t grid, uint32_t block,
                                 cudaStream_t stream);
 
+// Region-ordered probe (hash_join.cu): the probe side grouped by the table
+// region of its first slot, slice by slice (tuples: slice * 2*sizeof(K)
+// bytes of scratch, region_scratch: ht_region_scratch_bytes), then probed in
+// that order so the active table region stays in L2.
+uint32_t ht_region_bits(uint64_t size, uint32_t entry_bytes);
+size_t ht_region_scratch_bytes(uint32_t region_bits);
+template <typename K>
+cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size,
+                                    const K *key, const K *pay, uint64_t len,
+                                    uint64_t *result, uint32_t grid, uint32_t block,
+                                    uint32_t region_bits, void *tuples,
+                                    uint32_t *region_scratch, uint64_t slice,
+                                    uint32_t sm_count, cudaStream_t stream);
+
 // ---- generator -------------------------------------------------------------
 template <typename K>
 cudaError_t launch_gen_primary_keys(K *keys, uint64_t n, uint64_t seed, K base,

@@ -562,6 +562,12 @@ class CudaHashJoin:
         _check(f(self.h, _ptr(join_attr), _ptr(payload_attr),
                  C.c_uint64(join_attr.numel()), _stream(stream)))
 
+    def set_probe_grouping(self, enable=True, slice_tuples=1 << 27):
+        """Probe-side grouping by table region (fi_cuda_hash_join_set_probe_grouping;
+        no counterpart in the reference): on by default."""
+        _check(lib().fi_cuda_hash_join_set_probe_grouping(
+            self.h, C.c_int(1 if enable else 0), C.c_uint64(slice_tuples)))
+
     def probe_sum(self, join_attr, payload_attr, result_set, stream=None):
         f = getattr(lib(), "fi_cuda_hash_join_probe_sum_" + _sfx(join_attr.dtype))
         _check(f(self.h, _ptr(join_attr), _ptr(payload_attr),

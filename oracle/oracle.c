@@ -348,21 +348,29 @@ static uint32_t log2_floor_u64(uint64_t x) {
                                                                                \
   /* No-partitioning perfect build/probe,                                      \
    * sql-ops/cpputils/no_partitioning_join.cpp:165-273 (the selective build    \
-   * skips null keys). */                                                      \
-  void or_ht_build_perfect_##SUF(or_tuple_##SUF *ht, const K *keys,            \
-                                 const K *pays, uint64_t len, int selective) { \
+   * skips null keys).  Keys outside [0, entries) are skipped, as the GPU      \
+   * library does; the reference indexes the table with them unchecked. */    \
+  void or_ht_build_perfect_##SUF(or_tuple_##SUF *ht, uint64_t entries,       \
+                                 const K *keys, const K *pays, uint64_t len,   \
+                                 int selective) {                              \
     for (uint64_t t = 0; t < len; ++t) {                                       \
       if (selective && keys[t] == (K)-1) continue;                             \
-      ht[keys[t]].key = keys[t];                                               \
-      ht[keys[t]].value = pays[t];                                             \
+      const uint64_t s = (uint64_t)(int64_t)keys[t];                           \
+      if (s >= entries) continue; /* the reference indexes out of bounds */    \
+      ht[s].key = keys[t];                                                     \
+      ht[s].value = pays[t];                                                   \
     }                                                                          \
   }                                                                            \
   uint64_t or_ht_probe_aggregate_perfect_##SUF(const or_tuple_##SUF *ht,       \
+                                               uint64_t entries,               \
                                                const K *keys, const K *pays,   \
                                                uint64_t len) {                 \
     uint64_t sum = 0;                                                          \
-    for (uint64_t t = 0; t < len; ++t)                                         \
-      if (ht[keys[t]].key == keys[t]) sum += (uint64_t)(int64_t)pays[t];       \
+    for (uint64_t t = 0; t < len; ++t) {                                       \
+      const uint64_t s = (uint64_t)(int64_t)keys[t];                           \
+      if (s < entries && ht[s].key == keys[t])                                 \
+        sum += (uint64_t)(int64_t)pays[t];                                     \
+    }                                                                          \
     return sum;                                                                \
   }
 

@@ -173,11 +173,11 @@ def ht_perfect_sum(build_key, build_pay, probe_key, probe_pay, entries,
     ht = np.full((entries, 2), -1, dt)
     sfx = _sfx(dt)
     getattr(lib(), "or_ht_build_perfect_" + sfx)(
-        _p(ht), _p(build_key), _p(build_pay), C.c_uint64(len(build_key)),
-        C.c_int(1 if selective else 0))
+        _p(ht), C.c_uint64(entries), _p(build_key), _p(build_pay),
+        C.c_uint64(len(build_key)), C.c_int(1 if selective else 0))
     f = getattr(lib(), "or_ht_probe_aggregate_perfect_" + sfx)
     f.restype = C.c_uint64
-    return f(_p(ht), _p(probe_key), _p(probe_pay),
+    return f(_p(ht), C.c_uint64(entries), _p(probe_key), _p(probe_pay),
              C.c_uint64(len(probe_key))), ht
 
 

@@ -208,6 +208,43 @@ def test_hash_join_linear_probing_windows(fi, oracle, ndt, tdt, size, n_b, n_p):
     assert got == exp
 
 
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["LinearProbing", "Perfect"])
+@pytest.mark.parametrize("slice_", [1 << 27, 1_000_003])
+def test_hash_join_grouped_probe(fi, oracle, ndt, tdt, scheme, slice_):
+    """Tables larger than a region (8 MB) probed by at least one probe per
+    slot are probed region by region (the probe side grouped slice by
+    slice): the sum equals the oracle's and the ungrouped probe's, also when
+    slices split the probe side, with duplicate build keys, misses, keys
+    beyond a perfect table and negative payloads."""
+    rng = np.random.default_rng(11 + (slice_ & 7))
+    size = 1 << 21 if ndt == np.int64 else 1 << 22  # 32 MB tables
+    n_b = size // 2 if scheme == "LinearProbing" else size - 7
+    if scheme == "LinearProbing":
+        r_key = rng.integers(0, size // 3, n_b).astype(ndt)  # duplicates
+    else:
+        r_key = rng.permutation(n_b).astype(ndt)
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    n_p = 3 * size + 12345
+    s_key = rng.integers(-5, size + 100, n_p).astype(ndt)
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    dk, dp = to_dev(s_key), to_dev(s_pay)
+    got = []
+    for grouping in (True, False):
+        ht = fi.HashTable(size, tdt)
+        hj = fi.CudaHashJoin(getattr(fi.HashingScheme, scheme), ht, (148, 512), (148, 512))
+        hj.set_probe_grouping(grouping, slice_)
+        hj.build(to_dev(r_key), to_dev(r_pay))
+        res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
+        hj.probe_sum(dk, dp, res)
+        got.append(int(to_host(res).astype(np.uint64).sum(dtype=np.uint64)))
+    if scheme == "LinearProbing":
+        exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    else:
+        exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got[0] == got[1] == exp
+
+
 def test_hash_join_selective_perfect(fi, oracle):
     n = 50000
     r_key = oracle.primary_keys(n, 3, np.int64, base=0)
