@@ -11,8 +11,9 @@
 //    calls no CUDA allocator and frees nothing that the GPU still reads.
 //  * admission: a request is admitted when its relations (when the server
 //    holds them) get a block of the slab.  Requests are admitted in arrival
-//    order, except that small joins may pass a large one that waits for
-//    memory; one larger than the whole slab fails with FI_ERR_CAPACITY.
+//    order within two queues, small joins first, so that they need not wait
+//    behind a large one that waits for memory; one larger than the whole
+//    slab fails with FI_ERR_CAPACITY.
 //  * loading: server-held relations (host or synthetic sources) are copied
 //    or generated: those of small joins at admission on a high-priority load
 //    stream (an event marks them ready), those of large joins on their
@@ -180,7 +181,8 @@ struct fi_join_server {
   bool stop = false;
   std::thread sched;
   uint64_t next_ticket = 1;
-  std::deque<Request *> pending;               // not yet admitted
+  std::deque<Request *> pending;               // not yet admitted (large)
+  std::deque<Request *> pending_small;         // not yet admitted (small)
   std::deque<Request *> small_q[2];            // admitted small, per key type
   std::deque<Request *> large_q;               // admitted large
   std::unordered_map<uint64_t, Request *> all; // every uncollected request
@@ -555,28 +557,16 @@ void fi_join_server::loop() {
   for (;;) {
     bool progress = false;
     const Clock::time_point t0 = Clock::now();
-    // Admission in arrival order.  When the oldest request waits for arena
-    // memory, the small joins among the next kAdmitWindow requests (a few MB
-    // each) may still take a block, so that they do not wait behind a large
-    // one; large requests keep their order, so none is passed over for good.
-    constexpr size_t kAdmitWindow = 64;
-    bool blocked = false;
-    size_t looked = 0;
-    for (auto it = pending.begin(); it != pending.end() && !fatal;) {
-      Request *r = *it;
-      if (blocked) {
-        if (++looked > kAdmitWindow) break;
-        if (r->req.build_len + r->req.probe_len > cfg.small_tuples) {
-          ++it;
-          continue;
-        }
-      }
-      if (admit(r)) {
-        it = pending.erase(it);
+    // Admission in arrival order within two queues: small joins (a few MB
+    // each, below small_tuples) and the rest.  Small joins are admitted
+    // first, each as soon as its block fits, so that they do not wait
+    // behind a large request that waits for arena memory; large requests
+    // keep their arrival order.
+    for (std::deque<Request *> *q : {&pending_small, &pending}) {
+      while (!q->empty() && !fatal) {
+        if (!admit(q->front())) break;
+        q->pop_front();
         progress = true;
-      } else {
-        blocked = true;
-        ++it;
       }
     }
     progress |= complete();
@@ -587,7 +577,8 @@ void fi_join_server::loop() {
     if (progress) stats.enqueue_us += us_between(t0, Clock::now());
     if (fatal) {
       // a CUDA error is sticky: fail everything that has not started
-      for (std::deque<Request *> *q : {&pending, &small_q[0], &small_q[1], &large_q})
+      for (std::deque<Request *> *q :
+           {&pending_small, &pending, &small_q[0], &small_q[1], &large_q})
         while (!q->empty()) {
           finish(q->front(), fatal);
           q->pop_front();
@@ -596,7 +587,7 @@ void fi_join_server::loop() {
     bool busy = false;
     for (Worker &w : workers) busy |= w.count > 0;
     for (Runner &r : runners) busy |= r.batch.busy();
-    const bool queued = !pending.empty() || !small_q[0].empty() ||
+    const bool queued = !pending.empty() || !pending_small.empty() || !small_q[0].empty() ||
                         !small_q[1].empty() || !large_q.empty();
     if (stop && !busy && !queued) break;
     if (!progress) {
@@ -769,7 +760,9 @@ extern "C" int fi_join_server_submit(fi_join_server *s, const fi_join_request *r
     }
     *ticket = s->next_ticket++;
     s->all[*ticket] = r;
-    s->pending.push_back(r);
+    (r->req.build_len + r->req.probe_len <= s->cfg.small_tuples ? s->pending_small
+                                                                 : s->pending)
+        .push_back(r);
     ++s->stats.submitted;
   }
   s->cv_work.notify_one();
