@@ -814,14 +814,14 @@ struct fi_cuda_hash_join {
   DevBuf group_tuples, group_counts;
 };
 
-// Probe sides of at least one probe per table slot, on tables larger than a
-// region (8 MB), are grouped by table region before probing.
+// Probe sides of at least one probe per 128-byte table line, on tables
+// larger than a region, are grouped by table region before probing.
 static bool use_grouping(const fi_cuda_hash_join *h, uint64_t len, uint32_t entry_bytes,
                          uint32_t *region_bits) {
   if (!h->grouping) return false;
   *region_bits = ht_region_bits(h->size, entry_bytes);
   const uint64_t slots = 1ull << (63 - __builtin_clzll(h->size));
-  return *region_bits > 0 && len >= slots;
+  return *region_bits > 0 && len * 128 >= slots * entry_bytes;
 }
 
 extern "C" int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj,

@@ -289,7 +289,10 @@ __global__ void ht_probe_grouped_kernel(const Tuple<K> *__restrict__ ht,
 
 // Region bits of a table: regions of at most kRegionBytes; 0 when the whole
 // table fits kRegionBytes (then the probe needs no grouping).
-constexpr uint64_t kRegionBytes = 8ull << 20;
+#ifndef FI_REGION_MB
+#define FI_REGION_MB 8
+#endif
+constexpr uint64_t kRegionBytes = (uint64_t)FI_REGION_MB << 20;
 constexpr uint32_t kMaxRegionBits = 12;
 
 uint32_t ht_region_bits(uint64_t size, uint32_t entry_bytes) {

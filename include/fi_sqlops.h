@@ -421,8 +421,8 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
                                       uint64_t result_len, fi_stream_t stream);
 
 /* Probe-side grouping of CudaHashJoin::probe_sum; no counterpart in the
- * reference.  A probe side of at least one probe per table slot on a table
- * larger than 8 MB is grouped, slice by slice, by the table region of each
+ * reference.  A probe side of at least one probe per 128-byte table line on
+ * a table larger than 8 MB is grouped, slice by slice, by the table region of each
  * probe's first slot before it is probed, so the active region stays in L2
  * (the sum is the same).  On by default with slices of 2^27 tuples; each
  * slice takes slice * tuple_bytes bytes of scratch that the handle keeps.
