@@ -171,20 +171,40 @@ constexpr uint32_t kRegionThreads = 512;
 constexpr uint32_t kRegionItems = 8;
 constexpr uint32_t kRegionTile = kRegionThreads * kRegionItems;
 
+// Region counts.  With few regions every warp counts into its own copy of
+// the counters (copies = warps; one copy for more than kPrivateRegions
+// regions), so 512 threads do not all collide on a few shared counters;
+// four keys per thread are loaded before they are counted.
+constexpr uint32_t kPrivateRegions = 256;
+
 template <typename K>
 __global__ void __launch_bounds__(kRegionThreads)
     region_histogram_kernel(const K *__restrict__ key, uint64_t len, int scheme,
                             uint32_t lg, uint64_t size, uint32_t shift,
-                            uint32_t regions, uint32_t *__restrict__ counts) {
-  extern __shared__ uint32_t rh[];
-  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x) rh[r] = 0;
+                            uint32_t regions, uint32_t copies,
+                            uint32_t *__restrict__ counts) {
+  extern __shared__ uint32_t rh[];  // [copies][regions]
+  for (uint32_t r = threadIdx.x; r < regions * copies; r += blockDim.x) rh[r] = 0;
   __syncthreads();
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd(&rh[probe_region(load_cs(key + i), scheme, lg, size, shift, regions)], 1u);
+  uint32_t *mine = rh + (copies > 1 ? (threadIdx.x >> 5) * regions : 0);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < len;
+       b += 4 * stride) {
+    K k[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u)
+      if (b + u * stride < len) k[u] = load_cs(key + b + u * stride);
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u)
+      if (b + u * stride < len)
+        atomicAdd(&mine[probe_region(k[u], scheme, lg, size, shift, regions)], 1u);
+  }
   __syncthreads();
-  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x)
-    if (rh[r]) atomicAdd(&counts[r], rh[r]);
+  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x) {
+    uint32_t c = 0;
+    for (uint32_t w = 0; w < copies; ++w) c += rh[w * regions + r];
+    if (c) atomicAdd(&counts[r], c);
+  }
 }
 
 // One CTA: exclusive scan of the region counts into the claim cursors.
@@ -231,7 +251,17 @@ __global__ void __launch_bounds__(kRegionThreads)
         v[u] = load_cs(pay + t0 + j);
       }
       rg[u] = act ? probe_region(k[u], scheme, lg, size, shift, regions) : 0u;
-      rk[u] = act ? atomicAdd(&toff[rg[u]], 1u) : 0u;
+      // lanes of a warp with the same region take one shared atomic: with
+      // tens of regions most of a warp's lanes share a few counters
+      const uint32_t am = __ballot_sync(kFullMask, act);
+      rk[u] = 0;
+      if (act) {
+        const uint32_t peers = __match_any_sync(am, rg[u]);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (lane_id() == leader) base = atomicAdd(&toff[rg[u]], __popc(peers));
+        rk[u] = __shfl_sync(am, base, leader) + __popc(peers & lanemask_lt());
+      }
     }
     __syncthreads();
     block_exclusive_scan_u32(toff, regions, scan_tmp);
@@ -333,9 +363,10 @@ cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size
     const uint64_t n = min(slice, len - s0);
     e = cudaMemsetAsync(counts, 0, regions * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
+    const uint32_t copies = regions <= kPrivateRegions ? kRegionThreads / 32 : 1;
     region_histogram_kernel<K><<<2 * sm_count, kRegionThreads,
-                                 regions * sizeof(uint32_t), stream>>>(
-        key + s0, n, scheme, lg, ht_size, shift, regions, counts);
+                                 (size_t)regions * copies * sizeof(uint32_t), stream>>>(
+        key + s0, n, scheme, lg, ht_size, shift, regions, copies, counts);
     region_scan_kernel<<<1, 1024, (regions + 33) * sizeof(uint32_t), stream>>>(
         counts, regions, cursors);
     region_scatter_kernel<K><<<2 * sm_count, kRegionThreads, scatter_smem, stream>>>(
