@@ -84,6 +84,14 @@ def parse():
     ap.add_argument("--ht-dim", default="0,256",
                     help="nopart workload: grid,block of build and probe (grid 0 "
                          "= 8 CTAs per SM)")
+    ap.add_argument("--probe-grouping", default="on", choices=["on", "off"],
+                    help="nopart workload: probe tuples grouped by table region "
+                         "before probing (the library's default) or probed in "
+                         "input order")
+    ap.add_argument("--build-grouping", default="on", choices=["on", "off"],
+                    help="nopart workload: build tuples grouped by table region "
+                         "before inserting (the library's default) or inserted "
+                         "in input order")
     ap.add_argument("--exchange-log2n", type=int, default=29,
                     help="exchange workload: int64 tuples one sender partitions "
                          "and sends")
@@ -1468,6 +1476,8 @@ def run_nopart(a):
     ht = fi.HashTable(size, dt)
     hj = fi.CudaHashJoin(scheme, ht, (grid, blk), (grid, blk),
                          is_selective=a.selectivity < 100)
+    hj.set_probe_grouping(a.probe_grouping == "on")
+    hj.set_build_grouping(a.build_grouping == "on")
     res = torch.zeros(grid * blk, dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream()
     init = getattr(fi.lib(), "fi_hash_table_init_" + ("int32" if tb == 8 else "int64"))
@@ -1520,6 +1530,8 @@ def run_nopart(a):
                                a.data_set, "int32" if tb == 8 else "int64", a.ht_scheme),
                            "build_tuples": nb, "probe_tuples": npr,
                            "hash_table_entries": size, "grid": grid, "block": blk,
+                           "probe_grouping": a.probe_grouping,
+                           "build_grouping": a.build_grouping,
                            "l2_flush": "none: probe input larger than L2"},
                 "phases": {"init_build": {"ms": build_ms,
                                           "gb_per_s": build_bytes / (build_ms / 1e3) / 1e9},

@@ -808,17 +808,21 @@ struct fi_cuda_hash_join {
   void *ht;
   uint64_t mem_len, size;
   uint32_t bg, bb, pg, pb;
-  // region-ordered probing: on by default, slices of probe_slice tuples
+  // region-ordered probing and building: on by default, slices of
+  // probe_slice / build_slice tuples; both share the scratch buffers
   bool grouping = true;
   uint64_t probe_slice = 1ull << 27;
+  bool build_grouping = true;
+  uint64_t build_slice = 1ull << 27;
   DevBuf group_tuples, group_counts;
 };
 
-// Probe sides of at least one probe per 128-byte table line, on tables
-// larger than a region, are grouped by table region before probing.
-static bool use_grouping(const fi_cuda_hash_join *h, uint64_t len, uint32_t entry_bytes,
-                         uint32_t *region_bits) {
-  if (!h->grouping) return false;
+// Probe (build) sides of at least one tuple per 128-byte table line, on
+// tables larger than a region, are grouped by table region before probing
+// (inserting).
+static bool use_grouping(const fi_cuda_hash_join *h, bool enabled, uint64_t len,
+                         uint32_t entry_bytes, uint32_t *region_bits) {
+  if (!enabled) return false;
   *region_bits = ht_region_bits(h->size, entry_bytes);
   const uint64_t slots = 1ull << (63 - __builtin_clzll(h->size));
   return *region_bits > 0 && len * 128 >= slots * entry_bytes;
@@ -834,6 +838,25 @@ extern "C" int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj,
     return set_error(FI_ERR_INVALID_ARGUMENT, "slice_tuples must be below 2^32");
   hj->grouping = enable != 0;
   if (enable) hj->probe_slice = slice_tuples;
+  return FI_OK;
+}
+
+// The grouping scratch starts with the device status word of its scatter.
+extern "C" int fi_cuda_hash_join_status(fi_cuda_hash_join *hj) {
+  if (!hj) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  return read_and_clear_status(hj->group_counts);
+}
+
+extern "C" int fi_cuda_hash_join_set_build_grouping(fi_cuda_hash_join *hj,
+                                                    int enable,
+                                                    uint64_t slice_tuples) {
+  if (!hj) return set_error(FI_ERR_INVALID_ARGUMENT, "null handle");
+  if (enable && slice_tuples == 0)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "slice_tuples must be at least 1");
+  if (slice_tuples >= 0xffffffffull)
+    return set_error(FI_ERR_INVALID_ARGUMENT, "slice_tuples must be below 2^32");
+  hj->build_grouping = enable != 0;
+  if (enable) hj->build_slice = slice_tuples;
   return FI_OK;
 }
 
@@ -893,6 +916,18 @@ static int hj_build_impl(fi_cuda_hash_join *h, const K *key, const K *pay,
   if (h->scheme == FI_HASHING_BUCKET_CHAINING ||
       (h->scheme == FI_HASHING_LINEAR_PROBING && h->selective))
     return set_error(FI_ERR_UNSUPPORTED, "hashing scheme not implemented");
+  uint32_t region_bits = 0;
+  if (len > 0 && use_grouping(h, h->build_grouping, len, 2 * sizeof(K), &region_bits)) {
+    const uint64_t slice = std::min(len, h->build_slice);
+    int rc = h->group_tuples.reserve(slice * 2 * sizeof(K), false);
+    if (!rc) rc = h->group_counts.reserve(ht_region_scratch_bytes(region_bits), true);
+    if (rc) return rc;
+    cudaError_t e = launch_ht_build_grouped<K>(
+        h->scheme == FI_HASHING_LINEAR_PROBING ? 1 : 0, h->selective, h->ht,
+        h->size, key, pay, len, h->bg, h->bb, region_bits, h->group_tuples.ptr,
+        (uint32_t *)h->group_counts.ptr, slice, (uint32_t)device_sm_count(), stream);
+    return e == cudaSuccess ? FI_OK : cuda_error(e, "hash table build");
+  }
   cudaError_t e = launch_ht_build<K>(
       h->scheme == FI_HASHING_LINEAR_PROBING ? 1 : 0, h->selective, h->ht,
       h->size, key, pay, len, h->bg, h->bb, stream);
@@ -910,10 +945,10 @@ static int hj_probe_impl(fi_cuda_hash_join *h, const K *key, const K *pay,
   if (h->scheme == FI_HASHING_BUCKET_CHAINING)
     return set_error(FI_ERR_UNSUPPORTED, "hashing scheme not implemented");
   uint32_t region_bits = 0;
-  if (len > 0 && use_grouping(h, len, 2 * sizeof(K), &region_bits)) {
+  if (len > 0 && use_grouping(h, h->grouping, len, 2 * sizeof(K), &region_bits)) {
     const uint64_t slice = std::min(len, h->probe_slice);
     int rc = h->group_tuples.reserve(slice * 2 * sizeof(K), false);
-    if (!rc) rc = h->group_counts.reserve(ht_region_scratch_bytes(region_bits), false);
+    if (!rc) rc = h->group_counts.reserve(ht_region_scratch_bytes(region_bits), true);
     if (rc) return rc;
     cudaError_t e = launch_ht_probe_grouped<K>(
         h->scheme == FI_HASHING_LINEAR_PROBING ? 1 : 0, h->ht, h->size, key, pay,

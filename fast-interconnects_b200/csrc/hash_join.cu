@@ -13,10 +13,12 @@
 // and payloads with evict-first loads, and keys outside [0, size) are skipped
 // by the perfect scheme instead of addressing out of bounds.
 //
-// Measured on B200 (Blanas: 16M x 256M int64, 1184 x 256 threads): linear
-// probing builds in 1.0 ms and probes in 11.1 ms (a 2^25-entry, 512 MB
-// table: one random access per probe, far beyond the 126 MB L2), perfect
-// hashing probes in 4.7 ms (16M + 1 entries).  Four tuples per thread with
+// Measured on B200 (Blanas: 16M x 256M int64, 1184 x 256 threads), in input
+// order: linear probing builds in 1.0 ms and probes in 11.1 ms (a
+// 2^25-entry, 512 MB table: one random access per probe, far beyond the
+// 126 MB L2), perfect hashing probes in 4.7 ms (16M + 1 entries); grouped by
+// table region (below, the default), the linear-probing build takes 0.79 ms
+// and the probe 5.0 ms, the perfect probe 3.4 ms.  In input order, four tuples per thread with
 // their table loads issued together made it no faster (11.7 ms), nor did
 // loading a window of 4 slots (64 B) per step instead of slot by slot (11.0
 // ms): the probe is bound by the rate of random HBM accesses (about 30 G/s
@@ -25,8 +27,11 @@
 // matters more: the hash masks with 2^floor(log2(size)) (as the reference
 // does), so a size that is not a power of two can fill the table to near
 // 1 (Kim, 128e6 keys in 2^27 slots: 27 ms per probe against 5.8 ms in 2^28).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
+#include "tma_scatter.cuh"
 
 namespace fi {
 
@@ -141,14 +146,21 @@ __global__ void ht_probe_perfect_kernel(const Tuple<K> *__restrict__ ht,
   result[gid] += sum;
 }
 
-// ---- region-ordered probing ------------------------------------------------
+// ---- region-ordered probing and building ---------------------------------
 // A table far larger than L2 is probed at random: every probe reaches HBM
 // (Blanas, 2^25 int64 slots: 24 G probes/s, 11 ms).  Grouping the probe
 // tuples by the table region their first slot lies in (the top region_bits
 // bits of the slot) and probing group by group keeps the active region
 // (a few MB) in L2, so the table is read from HBM about once per slice.  The
-// grouping is one streamed pass (a histogram of region ids and a tile
-// scatter into a scratch buffer); the sum does not depend on the order.
+// grouping is one streamed pass: per-(chunk, region) counts, their scan, and
+// the TMA tile scatter of tma_scatter.cuh by region into a scratch buffer
+// (one chunk per SM; a per-tile variant with one global claim per (tile,
+// region) run serves columns that are not 16-byte aligned).  The sum does
+// not depend on the order.  The build side is grouped the same way, so the
+// table lines that inserts write stay in L2 until their region is done.
+// Measured on B200, per 128M int64 probes into a 512 MB table: counts 0.23
+// ms, scatter 0.92 ms (0.71 of the copy peak; 1.42 ms with the per-tile
+// claims), probe 1.17 ms.
 
 // Slot of a probe's first access: the hash (linear probing) or the key
 // (perfect; keys outside [0, size) probe nothing and go to the last region).
@@ -285,8 +297,120 @@ __global__ void __launch_bounds__(kRegionThreads)
   }
 }
 
+// The same grouping in chunks, without global atomics in the scatter: every
+// CTA of the TMA tile scatter (tma_scatter.cuh) owns one contiguous chunk of
+// the slice and writes its run of each region at a cursor fixed by a
+// per-(chunk, region) histogram.  The output is region-major (region r holds
+// chunk 0's tuples of r, then chunk 1's, ...).
+template <typename K>
+struct RegionOf {
+  int scheme;
+  uint32_t lg;
+  uint64_t size;
+  uint32_t shift, regions;
+  __device__ __forceinline__ uint32_t operator()(K k) const {
+    return probe_region(k, scheme, lg, size, shift, regions);
+  }
+};
+
+// Per-(chunk, region) counts into counts[chunk][regions] (zero on entry);
+// `per_chunk` CTAs share a chunk, four loads per thread in flight.
+template <typename K>
+__global__ void __launch_bounds__(kRegionThreads)
+    region_chunk_histogram_kernel(const K *__restrict__ key, uint64_t len,
+                                  uint64_t clen, uint32_t chunks,
+                                  uint32_t per_chunk, RegionOf<K> part,
+                                  uint32_t copies, uint32_t *__restrict__ counts) {
+  extern __shared__ uint32_t rh[];  // [copies][regions]
+  const uint32_t regions = part.regions;
+  for (uint32_t r = threadIdx.x; r < regions * copies; r += blockDim.x) rh[r] = 0;
+  __syncthreads();
+  const uint32_t c = blockIdx.x / per_chunk, sub = blockIdx.x % per_chunk;
+  const uint64_t cb = clen * c, ce = (c + 1 == chunks) ? len : cb + clen;
+  uint32_t *mine = rh + (copies > 1 ? (threadIdx.x >> 5) * regions : 0);
+  const uint64_t stride = (uint64_t)per_chunk * blockDim.x;
+  for (uint64_t b = cb + (uint64_t)sub * blockDim.x + threadIdx.x; b < ce;
+       b += 4 * stride) {
+    K k[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u)
+      if (b + u * stride < ce) k[u] = load_cs(key + b + u * stride);
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u)
+      if (b + u * stride < ce) atomicAdd(&mine[part(k[u])], 1u);
+  }
+  __syncthreads();
+  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x) {
+    uint32_t t = 0;
+    for (uint32_t w = 0; w < copies; ++w) t += rh[w * regions + r];
+    if (t) atomicAdd(&counts[(uint64_t)c * regions + r], t);
+  }
+}
+
+// One CTA: cursors[c][r] = (tuples of regions < r) + (tuples of region r in
+// chunks < c), the region-major start of chunk c's run of region r.
+__global__ void __launch_bounds__(1024)
+    region_chunk_scan_kernel(const uint32_t *__restrict__ counts, uint32_t chunks,
+                             uint32_t regions, uint64_t *__restrict__ cursors) {
+  extern __shared__ uint32_t tot[];  // [regions] + 33
+  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x) {
+    uint32_t t = 0;
+    for (uint32_t c = 0; c < chunks; ++c) t += counts[(uint64_t)c * regions + r];
+    tot[r] = t;
+  }
+  __syncthreads();
+  block_exclusive_scan_u32(tot, regions, tot + regions);
+  for (uint32_t r = threadIdx.x; r < regions; r += blockDim.x) {
+    uint64_t run = tot[r];
+    for (uint32_t c = 0; c < chunks; ++c) {
+      cursors[(uint64_t)c * regions + r] = run;
+      run += counts[(uint64_t)c * regions + r];
+    }
+  }
+}
+
+// The TMA tile scatter of chunk blockIdx.x by region.  Shared memory as
+// tma_tile_scatter_kernel's: bars | stages | toff | cur | scan_tmp.
+template <typename K>
+__global__ void __launch_bounds__(TmaShape<K>::kThreads, 1)
+    region_tma_scatter_kernel(const K *__restrict__ keys, const K *__restrict__ pays,
+                              uint64_t len, uint64_t clen, uint32_t chunks,
+                              RegionOf<K> part, const uint64_t *__restrict__ cursors,
+                              Tuple<K> *__restrict__ out, uint64_t out_len,
+                              int *status) {
+  using S = TmaShape<K>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t F = part.regions;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *stages = smem_raw + 64;
+  uint32_t *toff =
+      reinterpret_cast<uint32_t *>(stages + S::kStages * tma_stage_bytes<K>());
+  uint32_t *cur = toff + F + 1;
+  uint32_t *scan_tmp = cur + F;
+  const uint32_t c = blockIdx.x;
+  const uint64_t cb = clen * c, ce = (c + 1 == chunks) ? len : cb + clen;
+  // region-major cursors never lie below the chunk's run of region 0
+  const uint64_t base = cursors[(uint64_t)c * F];
+  for (uint32_t p = threadIdx.x; p < F; p += blockDim.x)
+    cur[p] = (uint32_t)(cursors[(uint64_t)c * F + p] - base);
+  for (uint32_t p = threadIdx.x; p <= F; p += blockDim.x) toff[p] = 0;
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < S::kStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  TmaColumnSource<K> src{keys, pays};
+  tma_tile_scatter_by<K, TmaColumnSource<K>, RegionOf<K>>(
+      src, cb, ce, F, part, cur, toff, scan_tmp, stages, bars, out, base, out_len,
+      status);
+}
+
 // The probes of a grouped slice, in order: every probe as in
-// ht_probe_{lp,perfect}_kernel.
+// ht_probe_{lp,perfect}_kernel.  (Four probes per thread with their first
+// table loads issued together measured slower, 1.17 -> 1.34 ms per 128M
+// int64 probes: 52 registers halve the resident threads, and the probe is
+// bound by the L1's one wavefront per uncoalesced slot load, not by the
+// L2 latency.)
 template <typename K>
 __global__ void ht_probe_grouped_kernel(const Tuple<K> *__restrict__ ht,
                                         uint64_t size, int scheme,
@@ -333,8 +457,81 @@ uint32_t ht_region_bits(uint64_t size, uint32_t entry_bytes) {
   return b;
 }
 
+// Region scratch: [status: one int, padded to kRegionStatusWords u32]
+// [counts: chunks x regions u32] [cursors: chunks x regions u64], with
+// chunks = the SM count (at most kMaxRegionChunks).  The status sits at the
+// start, so it stays in place whatever region count later calls use.  The
+// per-tile path uses 2 x regions u32 after the status.
 size_t ht_region_scratch_bytes(uint32_t region_bits) {
-  return ((size_t)2 << region_bits) * sizeof(uint32_t);
+  return kRegionStatusWords * sizeof(uint32_t) +
+         ((size_t)kMaxRegionChunks << region_bits) * (sizeof(uint32_t) + sizeof(uint64_t));
+}
+
+// Groups tuples [0, n) of the two columns by table region into `out`
+// (region order; the order inside a region is the order in which tiles claim
+// their runs): region counts, their scan, and the tile scatter.
+template <typename K>
+static cudaError_t group_by_region(int scheme, uint64_t ht_size, const K *key,
+                                   const K *pay, uint64_t n, uint32_t region_bits,
+                                   Tuple<K> *out, uint32_t *region_scratch,
+                                   uint32_t sm_count, cudaStream_t stream) {
+  const uint32_t lg = 63u - (uint32_t)__builtin_clzll(ht_size);
+  const uint32_t regions = 1u << region_bits;
+  // linear probing: regions of the hash range 2^lg; perfect: of the key
+  // range [0, size), rounded up to a power of two
+  uint32_t range_bits = lg;
+  if (scheme != 1 && (1ull << lg) < ht_size) ++range_bits;
+  const uint32_t shift = range_bits > region_bits ? range_bits - region_bits : 0;
+  // chunked TMA path: 16-byte aligned columns, the scatter's shared memory
+  // within the opt-in limit, one chunk per SM
+  const size_t tma_sm = tma_scatter_smem<K>(regions);
+  const uint32_t chunks = std::min<uint32_t>(sm_count, kMaxRegionChunks);
+  if (((reinterpret_cast<uintptr_t>(key) | reinterpret_cast<uintptr_t>(pay)) % 16) == 0 &&
+      tma_sm <= (size_t)device_max_smem_optin() && chunks > 0) {
+    const RegionOf<K> part{scheme, lg, ht_size, shift, regions};
+    int *status = reinterpret_cast<int *>(region_scratch);
+    uint32_t *counts = region_scratch + kRegionStatusWords;
+    uint64_t *cursors = reinterpret_cast<uint64_t *>(
+        counts + ((size_t)kMaxRegionChunks << region_bits));
+    // chunk starts on 128-byte boundaries; the last chunk takes the rest
+    constexpr uint64_t kAlignMask = ~((uint64_t)(kAlignBytes / sizeof(K)) - 1ull);
+    const uint64_t clen = ((n + chunks - 1) / chunks) & kAlignMask;
+    cudaError_t e = cudaFuncSetAttribute((const void *)region_tma_scatter_kernel<K>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tma_sm);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(counts, 0, (size_t)chunks * regions * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    const uint32_t copies = regions <= kPrivateRegions ? kRegionThreads / 32 : 1;
+    const uint32_t per_chunk = 2;
+    region_chunk_histogram_kernel<K><<<chunks * per_chunk, kRegionThreads,
+                                       (size_t)regions * copies * sizeof(uint32_t),
+                                       stream>>>(key, n, clen, chunks, per_chunk, part,
+                                                 copies, counts);
+    region_chunk_scan_kernel<<<1, 1024, (regions + 33) * sizeof(uint32_t), stream>>>(
+        counts, chunks, regions, cursors);
+    region_tma_scatter_kernel<K><<<chunks, TmaShape<K>::kThreads, tma_sm, stream>>>(
+        key, pay, n, clen, chunks, part, cursors, out, n, status);
+    return cudaGetLastError();
+  }
+  uint32_t *counts = region_scratch + kRegionStatusWords, *cursors = counts + regions;
+  const size_t scatter_smem = (size_t)kRegionTile * sizeof(Tuple<K>) +
+                              ((size_t)2 * regions + 1 + 33) * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute((const void *)region_scatter_kernel<K>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)scatter_smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(counts, 0, regions * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  const uint32_t copies = regions <= kPrivateRegions ? kRegionThreads / 32 : 1;
+  region_histogram_kernel<K><<<2 * sm_count, kRegionThreads,
+                               (size_t)regions * copies * sizeof(uint32_t), stream>>>(
+      key, n, scheme, lg, ht_size, shift, regions, copies, counts);
+  region_scan_kernel<<<1, 1024, (regions + 33) * sizeof(uint32_t), stream>>>(
+      counts, regions, cursors);
+  region_scatter_kernel<K><<<2 * sm_count, kRegionThreads, scatter_smem, stream>>>(
+      key, pay, n, scheme, lg, ht_size, shift, regions, cursors, out);
+  return cudaGetLastError();
 }
 
 template <typename K>
@@ -344,35 +541,59 @@ cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size
                                     uint32_t region_bits, void *tuples,
                                     uint32_t *region_scratch, uint64_t slice,
                                     uint32_t sm_count, cudaStream_t stream) {
-  const uint32_t lg = 63u - (uint32_t)__builtin_clzll(ht_size);
-  const uint32_t regions = 1u << region_bits;
-  // linear probing: regions of the hash range 2^lg; perfect: of the key
-  // range [0, size), rounded up to a power of two
-  uint32_t range_bits = lg;
-  if (scheme != 1 && (1ull << lg) < ht_size) ++range_bits;
-  const uint32_t shift = range_bits > region_bits ? range_bits - region_bits : 0;
-  uint32_t *counts = region_scratch, *cursors = region_scratch + regions;
   Tuple<K> *out = static_cast<Tuple<K> *>(tuples);
-  const size_t scatter_smem = (size_t)kRegionTile * sizeof(Tuple<K>) +
-                              ((size_t)2 * regions + 1 + 33) * sizeof(uint32_t);
-  cudaError_t e = cudaFuncSetAttribute((const void *)region_scatter_kernel<K>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)scatter_smem);
-  if (e != cudaSuccess) return e;
   for (uint64_t s0 = 0; s0 < len; s0 += slice) {
     const uint64_t n = min(slice, len - s0);
-    e = cudaMemsetAsync(counts, 0, regions * sizeof(uint32_t), stream);
+    cudaError_t e = group_by_region<K>(scheme, ht_size, key + s0, pay + s0, n,
+                                       region_bits, out, region_scratch, sm_count,
+                                       stream);
     if (e != cudaSuccess) return e;
-    const uint32_t copies = regions <= kPrivateRegions ? kRegionThreads / 32 : 1;
-    region_histogram_kernel<K><<<2 * sm_count, kRegionThreads,
-                                 (size_t)regions * copies * sizeof(uint32_t), stream>>>(
-        key + s0, n, scheme, lg, ht_size, shift, regions, copies, counts);
-    region_scan_kernel<<<1, 1024, (regions + 33) * sizeof(uint32_t), stream>>>(
-        counts, regions, cursors);
-    region_scatter_kernel<K><<<2 * sm_count, kRegionThreads, scatter_smem, stream>>>(
-        key + s0, pay + s0, n, scheme, lg, ht_size, shift, regions, cursors, out);
     ht_probe_grouped_kernel<K><<<grid, block, 0, stream>>>(
         static_cast<const Tuple<K> *>(ht), ht_size, scheme, out, n, result);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Inserts of a grouped slice, in order: every insert as in
+// ht_build_{lp,perfect}_kernel.  Consecutive threads insert tuples of one
+// region, so the lines they write stay in L2 until the region is done.
+template <typename K>
+__global__ void ht_build_grouped_kernel(Tuple<K> *ht, uint64_t size, int scheme,
+                                        bool selective,
+                                        const Tuple<K> *__restrict__ tuples,
+                                        uint64_t len) {
+  const uint32_t lg = log2_floor_u64(size);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const Tuple<K> t = load_tuple_cs(tuples + i);
+    if (scheme == 1) {
+      lp_insert(ht, lg, t.key, t.value);
+    } else {
+      if (selective && t.key == null_key<K>()) continue;
+      const uint64_t slot = static_cast<uint64_t>(static_cast<int64_t>(t.key));
+      if (slot < size) store_tuple(ht + slot, t);
+    }
+  }
+}
+
+template <typename K>
+cudaError_t launch_ht_build_grouped(int scheme, bool selective, void *ht,
+                                    uint64_t ht_size, const K *key, const K *pay,
+                                    uint64_t len, uint32_t grid, uint32_t block,
+                                    uint32_t region_bits, void *tuples,
+                                    uint32_t *region_scratch, uint64_t slice,
+                                    uint32_t sm_count, cudaStream_t stream) {
+  Tuple<K> *out = static_cast<Tuple<K> *>(tuples);
+  for (uint64_t s0 = 0; s0 < len; s0 += slice) {
+    const uint64_t n = min(slice, len - s0);
+    cudaError_t e = group_by_region<K>(scheme, ht_size, key + s0, pay + s0, n,
+                                       region_bits, out, region_scratch, sm_count,
+                                       stream);
+    if (e != cudaSuccess) return e;
+    ht_build_grouped_kernel<K><<<grid, block, 0, stream>>>(
+        static_cast<Tuple<K> *>(ht), ht_size, scheme, selective, out, n);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -422,6 +643,9 @@ cudaError_t launch_ht_probe_sum(int scheme, const void *ht, uint64_t ht_size,
       int, const void *, uint64_t, const K *, const K *, uint64_t, uint64_t *, \
       uint32_t, uint32_t, uint32_t, void *, uint32_t *, uint64_t, uint32_t,    \
       cudaStream_t);                                                           \
+  template cudaError_t launch_ht_build_grouped<K>(                             \
+      int, bool, void *, uint64_t, const K *, const K *, uint64_t, uint32_t,   \
+      uint32_t, uint32_t, void *, uint32_t *, uint64_t, uint32_t, cudaStream_t); \
   template cudaError_t launch_ht_init<K>(void *, uint64_t, cudaStream_t);      \
   template cudaError_t launch_ht_build<K>(int, bool, void *, uint64_t,         \
                                           const K *, const K *, uint64_t,      \

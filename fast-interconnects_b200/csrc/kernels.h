@@ -149,12 +149,26 @@ cudaError_t launch_ht_probe_sum(int scheme, const void *ht, uint64_t ht_size,
 // region of its first slot, slice by slice (tuples: slice * 2*sizeof(K)
 // bytes of scratch, region_scratch: ht_region_scratch_bytes), then probed in
 // that order so the active table region stays in L2.
+// The scratch starts with a device status word (FI_ERR_TIMEOUT when a bounded
+// wait of the grouping scatter gave up), padded to kRegionStatusWords u32;
+// grouping runs one chunk per SM, for at most kMaxRegionChunks SMs.
+constexpr uint32_t kRegionStatusWords = 64;
+constexpr uint32_t kMaxRegionChunks = 256;
 uint32_t ht_region_bits(uint64_t size, uint32_t entry_bytes);
 size_t ht_region_scratch_bytes(uint32_t region_bits);
 template <typename K>
 cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size,
                                     const K *key, const K *pay, uint64_t len,
                                     uint64_t *result, uint32_t grid, uint32_t block,
+                                    uint32_t region_bits, void *tuples,
+                                    uint32_t *region_scratch, uint64_t slice,
+                                    uint32_t sm_count, cudaStream_t stream);
+// Region-ordered build: the build side grouped the same way, slice by slice,
+// then inserted in that order so the lines being written stay in L2.
+template <typename K>
+cudaError_t launch_ht_build_grouped(int scheme, bool selective, void *ht,
+                                    uint64_t ht_size, const K *key, const K *pay,
+                                    uint64_t len, uint32_t grid, uint32_t block,
                                     uint32_t region_bits, void *tuples,
                                     uint32_t *region_scratch, uint64_t slice,
                                     uint32_t sm_count, cudaStream_t stream);

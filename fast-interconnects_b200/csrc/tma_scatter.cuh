@@ -205,10 +205,21 @@ struct TmaRegionSource {
 // so no separate staging buffer is needed and the stages can be 50% longer.
 // Called once per barrier initialisation by all threads; thread 0 issues
 // the copies.
-template <typename K, typename Src, bool kUniformWarps = false>
-__device__ __forceinline__ void tma_tile_scatter_range(
-    Src &src, uint64_t begin, uint64_t end, uint32_t F, uint64_t mask,
-    uint32_t ignore_bits, uint32_t *cur, uint32_t *toff, uint32_t *warp_tmp,
+// The partition of a key: its radix digit (key_to_partition).
+template <typename K>
+struct RadixDigit {
+  uint64_t mask;
+  uint32_t ignore_bits;
+  __device__ __forceinline__ uint32_t operator()(K k) const {
+    return key_to_partition(k, mask, ignore_bits);
+  }
+};
+
+// The scatter for any partition function `part` (key -> [0, F)).
+template <typename K, typename Src, typename Part, bool kUniformWarps = false>
+__device__ __forceinline__ void tma_tile_scatter_by(
+    Src &src, uint64_t begin, uint64_t end, uint32_t F, const Part part,
+    uint32_t *cur, uint32_t *toff, uint32_t *warp_tmp,
     unsigned char *stages, uint64_t *bars, Tuple<K> *__restrict__ out,
     uint64_t cur_base, uint64_t out_len, int *status) {
   using S = TmaShape<K>;
@@ -247,7 +258,7 @@ __device__ __forceinline__ void tma_tile_scatter_range(
       const uint32_t i = u * T + tid;
       const bool act = ok && i < n_valid;
       if (act) src.get(stage, t0, n_valid, i, ck[u], cv[u]);
-      pp[u] = act ? key_to_partition(ck[u], mask, ignore_bits) : 0u;
+      pp[u] = act ? part(ck[u]) : 0u;
       rk[u] = kUniformWarps ? warp_uniform_rank(toff, pp[u], act)
                             : warp_aggregated_rank(toff, pp[u], act);
     }
@@ -283,7 +294,7 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     // 4. write the runs: tuple j of run p goes to cur[p] + (j - toff[p])
     for (uint32_t j = tid; j < n_valid; j += T) {
       const Tuple<K> tp = staged[j];
-      const uint32_t p = key_to_partition(tp.key, mask, ignore_bits);
+      const uint32_t p = part(tp.key);
       const uint64_t dst = cur_base + (uint32_t)(cur[p] + (j - toff[p]));
       if (dst < out_len)
         store_tuple(out + dst, tp);
@@ -301,6 +312,18 @@ __device__ __forceinline__ void tma_tile_scatter_range(
     for (uint32_t p = tid; p <= F; p += T) toff[p] = 0;
     __syncthreads();
   }
+}
+
+// The scatter by the radix digit (mask, ignore_bits).
+template <typename K, typename Src, bool kUniformWarps = false>
+__device__ __forceinline__ void tma_tile_scatter_range(
+    Src &src, uint64_t begin, uint64_t end, uint32_t F, uint64_t mask,
+    uint32_t ignore_bits, uint32_t *cur, uint32_t *toff, uint32_t *warp_tmp,
+    unsigned char *stages, uint64_t *bars, Tuple<K> *__restrict__ out,
+    uint64_t cur_base, uint64_t out_len, int *status) {
+  tma_tile_scatter_by<K, Src, RadixDigit<K>, kUniformWarps>(
+      src, begin, end, F, RadixDigit<K>{mask, ignore_bits}, cur, toff, warp_tmp,
+      stages, bars, out, cur_base, out_len, status);
 }
 
 }  // namespace fi

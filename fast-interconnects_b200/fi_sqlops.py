@@ -568,6 +568,18 @@ class CudaHashJoin:
         _check(lib().fi_cuda_hash_join_set_probe_grouping(
             self.h, C.c_int(1 if enable else 0), C.c_uint64(slice_tuples)))
 
+    def set_build_grouping(self, enable=True, slice_tuples=1 << 27):
+        """Build-side grouping by table region (fi_cuda_hash_join_set_build_grouping;
+        no counterpart in the reference): on by default."""
+        _check(lib().fi_cuda_hash_join_set_build_grouping(
+            self.h, C.c_int(1 if enable else 0), C.c_uint64(slice_tuples)))
+
+    def status(self):
+        """Raises the device-side error (a bounded wait that gave up) of the
+        grouped build and probe since the last call
+        (fi_cuda_hash_join_status)."""
+        _check(lib().fi_cuda_hash_join_status(self.h))
+
     def probe_sum(self, join_attr, payload_attr, result_set, stream=None):
         f = getattr(lib(), "fi_cuda_hash_join_probe_sum_" + _sfx(join_attr.dtype))
         _check(f(self.h, _ptr(join_attr), _ptr(payload_attr),

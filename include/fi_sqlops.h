@@ -430,6 +430,25 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
 int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj, int enable,
                                          uint64_t slice_tuples);
 
+/* Build-side grouping of CudaHashJoin::build; no counterpart in the
+ * reference.  The same grouping for the build: a build side of at least one
+ * tuple per 128-byte table line on a table larger than 8 MB is grouped, slice
+ * by slice, by the table region of each tuple's first slot before it is
+ * inserted, so the lines being written stay in L2.  The probe sums are the
+ * same; with linear probing the slots that equal keys occupy may differ from
+ * an ungrouped build, as they may between any two concurrent builds.  On by
+ * default with slices of 2^27 tuples, sharing the probe's scratch (the larger
+ * of the two slices is kept).  enable = 0 inserts in input order with no
+ * scratch. */
+int fi_cuda_hash_join_set_build_grouping(fi_cuda_hash_join *hj, int enable,
+                                         uint64_t slice_tuples);
+
+/* Device-side errors of the grouped build and probe; no counterpart in the
+ * reference, whose kernels have no bounded waits.  Synchronises the device,
+ * then returns FI_ERR_TIMEOUT if a bounded wait of a grouping scatter gave
+ * up since the last call (and clears it), else FI_OK. */
+int fi_cuda_hash_join_status(fi_cuda_hash_join *hj);
+
 /* ---- CpuHashJoin: no-partitioning join on the host
  *      (sql-ops/src/join/no_partitioning_join.rs:281-304, impl :440-560;
  *      kernels sql-ops/cpputils/no_partitioning_join.cpp:27-273) -------- */

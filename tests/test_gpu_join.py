@@ -237,11 +237,55 @@ def test_hash_join_grouped_probe(fi, oracle, ndt, tdt, scheme, slice_):
         hj.build(to_dev(r_key), to_dev(r_pay))
         res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
         hj.probe_sum(dk, dp, res)
+        hj.status()
         got.append(int(to_host(res).astype(np.uint64).sum(dtype=np.uint64)))
     if scheme == "LinearProbing":
         exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
     else:
         exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got[0] == got[1] == exp
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme,selective", [("LinearProbing", False),
+                                              ("Perfect", False), ("Perfect", True)])
+@pytest.mark.parametrize("slice_", [1 << 27, 333_331])
+def test_hash_join_grouped_build(fi, oracle, ndt, tdt, scheme, selective, slice_):
+    """Build sides of at least one tuple per 128-byte table line are inserted
+    region by region (grouped slice by slice): the probe sums equal the
+    oracle's and those of a build in input order, with duplicate build keys
+    (linear probing), null and out-of-range build keys (perfect), misses and
+    negative payloads, also when slices split the build side."""
+    rng = np.random.default_rng(23 + (slice_ & 7) + 2 * selective)
+    size = 1 << 21 if ndt == np.int64 else 1 << 22  # 32 MB tables
+    if scheme == "LinearProbing":
+        n_b = size // 2
+        r_key = rng.integers(0, size // 3, n_b).astype(ndt)  # duplicates
+    else:
+        n_b = size - 9
+        r_key = rng.permutation(n_b).astype(ndt)
+        r_key[::11] = -1  # the null key: skipped by the selective build
+        r_key[5::97] = size + 3  # beyond the table: skipped
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    n_p = size + 4321
+    s_key = rng.integers(-5, size + 100, n_p).astype(ndt)
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    rk, rp, dk, dp = to_dev(r_key), to_dev(r_pay), to_dev(s_key), to_dev(s_pay)
+    got = []
+    for grouping in (True, False):
+        ht = fi.HashTable(size, tdt)
+        hj = fi.CudaHashJoin(getattr(fi.HashingScheme, scheme), ht, (148, 512),
+                             (148, 512), is_selective=selective)
+        hj.set_build_grouping(grouping, slice_)
+        hj.build(rk, rp)
+        res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
+        hj.probe_sum(dk, dp, res)
+        hj.status()
+        got.append(int(to_host(res).astype(np.uint64).sum(dtype=np.uint64)))
+    if scheme == "LinearProbing":
+        exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    else:
+        exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size, selective)
     assert got[0] == got[1] == exp
 
 
