@@ -150,7 +150,9 @@ cudaError_t launch_ht_probe_sum(int scheme, const void *ht, uint64_t ht_size,
 // bytes of scratch, region_scratch: ht_region_scratch_bytes), then probed in
 // that order so the active table region stays in L2.
 // The scratch starts with a device status word (FI_ERR_TIMEOUT when a bounded
-// wait of the grouping scatter gave up), padded to kRegionStatusWords u32;
+// wait of the grouping scatter gave up; word 1 is the in-order build's tile
+// counter, word 2 the probe's "slice left in input order" flag), padded to
+// kRegionStatusWords u32;
 // grouping runs one chunk per SM, for at most kMaxRegionChunks SMs.
 constexpr uint32_t kRegionStatusWords = 64;
 constexpr uint32_t kMaxRegionChunks = 256;

@@ -476,7 +476,12 @@ static cudaError_t launch_wide_histogram(const K *keys, const K *pays,
   // measured on B200, 512M keys over 148 chunks: at 2^16 bins the two-range
   // kernel takes 2.0 ms and the cluster 3.0 ms (its remote shared-memory
   // atomics cost more than the second, mostly L2-served, key read); at 2^18
-  // bins eight reads per key make the ranges slower (7.8 ms vs 7.0 ms)
+  // bins eight reads per key make the ranges slower (7.8 ms vs 7.0 ms).  One
+  // global reduction per key into the chunk's histogram, CTAs taking tiles
+  // in input order so that one or two chunks' histograms (1 MB each) take
+  // the reductions from L2, measured slower still: 8.1 ms at 2^17 and 8.2
+  // ms at 2^18 bins for uniform keys, 10.3-11.7 ms for Zipf 1.0-1.5 keys
+  // (the hot bin's reductions serialise in one L2 slice)
   if (dst_key == nullptr && ranges == 8) {
     const size_t csm = (size_t)sizeof(uint32_t) << kHistSmemBinsLog2;
     cudaError_t e = cudaFuncSetAttribute(

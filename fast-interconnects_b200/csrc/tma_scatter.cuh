@@ -104,6 +104,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 }
 
 
+// Bounded waits for the copies of tiles t and t+1 (if any), the ones a CTA
+// may still have in flight when a wait gave up.  Out of line: inlined into
+// the scatter, the error path made the second-pass kernel spill registers
+// (4% slower).
+template <uint32_t kStages>
+__device__ __noinline__ void tma_drain(uint64_t *bars, uint64_t t, uint64_t ntiles) {
+  const uint64_t last = t + 2 < ntiles ? t + 2 : ntiles;
+  for (uint64_t tt = t; tt < last; ++tt)
+    for (uint32_t round = 0;
+         round < 4 && !mbar_wait(&bars[tt % kStages], (uint32_t)((tt / kStages) & 1u));
+         ++round) {
+    }
+}
+
 template <typename K>
 struct TmaShape {
   static constexpr uint32_t kThreads = 1024;
@@ -271,14 +285,7 @@ __device__ __forceinline__ void tma_tile_scatter_by(
         // for both copies this CTA may still have in flight, tile t's (whose
         // wait gave up) and tile t+1's.  A copy that outlasts these waits as
         // well is reported by the timeout status above.
-        for (uint32_t round = 0; round < 4 && !mbar_wait(&bars[s], parity); ++round) {
-        }
-        if (t + 1 < ntiles) {
-          const uint32_t s1 = (uint32_t)((t + 1) % S::kStages);
-          const uint32_t p1 = (uint32_t)(((t + 1) / S::kStages) & 1u);
-          for (uint32_t round = 0; round < 4 && !mbar_wait(&bars[s1], p1); ++round) {
-          }
-        }
+        tma_drain<S::kStages>(bars, t, ntiles);
       }
       __syncthreads();
       return;

@@ -424,8 +424,11 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
  * reference.  A probe side of at least one probe per 128-byte table line on
  * a table larger than 8 MB is grouped, slice by slice, by the table region of each
  * probe's first slot before it is probed, so the active region stays in L2
- * (the sum is the same).  On by default with slices of 2^27 tuples; each
- * slice takes slice * tuple_bytes bytes of scratch that the handle keeps.
+ * (the sum is the same).  A slice whose largest region would hold more than
+ * a quarter of its probes (heavy skew, whose probes already share a few
+ * table lines) is probed in input order; the device decides per slice, with
+ * no host round trip.  On by default with slices of 2^27 tuples; each slice
+ * takes slice * tuple_bytes bytes of scratch that the handle keeps.
  * enable = 0 probes in input order with no scratch. */
 int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj, int enable,
                                          uint64_t slice_tuples);
@@ -436,10 +439,12 @@ int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj, int enable,
  * by slice, by the table region of each tuple's first slot before it is
  * inserted, so the lines being written stay in L2.  The probe sums are the
  * same; with linear probing the slots that equal keys occupy may differ from
- * an ungrouped build, as they may between any two concurrent builds.  On by
+ * an ungrouped build, as they may between any two concurrent builds.  The
+ * grouped inserts run with the library's own launch shape (blocks take
+ * tiles of the grouped slice in order), not the handle's build grid.  On by
  * default with slices of 2^27 tuples, sharing the probe's scratch (the larger
  * of the two slices is kept).  enable = 0 inserts in input order with no
- * scratch. */
+ * scratch, on the build grid. */
 int fi_cuda_hash_join_set_build_grouping(fi_cuda_hash_join *hj, int enable,
                                          uint64_t slice_tuples);
 

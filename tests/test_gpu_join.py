@@ -247,6 +247,70 @@ def test_hash_join_grouped_probe(fi, oracle, ndt, tdt, scheme, slice_):
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["LinearProbing", "Perfect"])
+@pytest.mark.parametrize("slice_", [1 << 27, 1_000_003])
+def test_hash_join_grouped_probe_skewed(fi, oracle, ndt, tdt, scheme, slice_):
+    """A probe slice whose largest table region holds more than a quarter of
+    it (here half the probes are one key) is probed in input order instead
+    of grouped; the sums equal the oracle's and the ungrouped probe's, also
+    when slices split the probe side (unaligned slices take the per-tile
+    grouping, which always groups)."""
+    rng = np.random.default_rng(5 + (slice_ & 3))
+    size = 1 << 21 if ndt == np.int64 else 1 << 22  # 32 MB tables
+    n_b = size // 2
+    r_key = rng.permutation(n_b).astype(ndt)
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    n_p = 2 * size + 999
+    s_key = rng.integers(-3, n_b + 10, n_p).astype(ndt)
+    s_key[rng.random(n_p) < 0.5] = 12345  # the hot key
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    dk, dp = to_dev(s_key), to_dev(s_pay)
+    got = []
+    for grouping in (True, False):
+        ht = fi.HashTable(size, tdt)
+        hj = fi.CudaHashJoin(getattr(fi.HashingScheme, scheme), ht, (148, 512), (148, 512))
+        hj.set_probe_grouping(grouping, slice_)
+        hj.build(to_dev(r_key), to_dev(r_pay))
+        res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
+        hj.probe_sum(dk, dp, res)
+        hj.status()
+        got.append(int(to_host(res).astype(np.uint64).sum(dtype=np.uint64)))
+    if scheme == "LinearProbing":
+        exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    else:
+        exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got[0] == got[1] == exp
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("offset", [0, 1])
+def test_hash_join_grouped_probe_table_alignment(fi, oracle, ndt, tdt, offset):
+    """The grouped linear-probing probe reads 32-byte windows of the table
+    when its base is 32-byte aligned and slot by slot otherwise (a table one
+    entry into its allocation): both give the oracle's sum, with duplicate
+    build keys, misses and a nearly half-full table."""
+    rng = np.random.default_rng(41 + offset)
+    size = 1 << 21 if ndt == np.int64 else 1 << 22  # 32 MB tables
+    n_b = size // 2
+    r_key = rng.integers(0, size // 3, n_b).astype(ndt)
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    n_p = 2 * size + 77
+    s_key = rng.integers(-3, size // 3 + 50, n_p).astype(ndt)
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    ht = fi.HashTable(size, tdt, mem_len=size + 1)
+    ht.mem = ht.mem[offset:offset + size]
+    assert (ht.mem.data_ptr() % 32 == 0) == (offset == 0)
+    hj = fi.CudaHashJoin(fi.HashingScheme.LinearProbing, ht, (148, 512), (148, 512))
+    hj.build(to_dev(r_key), to_dev(r_pay))
+    res = torch.zeros(148 * 512, dtype=torch.int64, device="cuda")
+    hj.probe_sum(to_dev(s_key), to_dev(s_pay), res)
+    hj.status()
+    got = int(to_host(res).astype(np.uint64).sum(dtype=np.uint64))
+    exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got == exp
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
 @pytest.mark.parametrize("scheme,selective", [("LinearProbing", False),
                                               ("Perfect", False), ("Perfect", True)])
 @pytest.mark.parametrize("slice_", [1 << 27, 333_331])
