@@ -428,7 +428,9 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
  * a quarter of its probes (heavy skew, whose probes already share a few
  * table lines) is probed in input order; the device decides per slice, with
  * no host round trip.  On by default with slices of 2^27 tuples; each slice
- * takes slice * tuple_bytes bytes of scratch that the handle keeps.
+ * takes slice * tuple_bytes bytes of scratch that the handle keeps, so
+ * builds and probes of one handle whose work overlaps on the GPU (different
+ * streams) race on it: order them, as the table itself requires.
  * enable = 0 probes in input order with no scratch. */
 int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj, int enable,
                                          uint64_t slice_tuples);

@@ -408,6 +408,16 @@ class CudaHashJoin {
     check(detail::Ops<K>::ht_probe_sum(hj_, key, pay, len, result_set, result_len,
                                        detail::st(stream)));
   }
+  // Region-ordered build and probe (no counterpart in the reference; on by
+  // default): fi_cuda_hash_join_set_{build,probe}_grouping.
+  void set_build_grouping(bool enable, uint64_t slice_tuples = 1ull << 27) {
+    check(fi_cuda_hash_join_set_build_grouping(hj_, enable ? 1 : 0, slice_tuples));
+  }
+  void set_probe_grouping(bool enable, uint64_t slice_tuples = 1ull << 27) {
+    check(fi_cuda_hash_join_set_probe_grouping(hj_, enable ? 1 : 0, slice_tuples));
+  }
+  // Throws on a device-side error of the grouped build or probe.
+  void status() { check(fi_cuda_hash_join_status(hj_)); }
 
  private:
   fi_cuda_hash_join *hj_ = nullptr;

@@ -7,6 +7,8 @@
 //  * the radix join known answer (sql-ops/tests/test_cuda_radix_join.rs:
 //    179-182): keys a permutation of 0..N-1 on both sides, payload = row + 1,
 //    SUM(s.value) = N (N + 1) / 2, for both hashing schemes;
+//  * the no-partitioning join, grouped by table region and in input order:
+//    SUM of probe payloads 1 = the number of probes, every key present;
 //  * the reference's argument check: mismatching radix bits raise
 //    ErrorKind::InvalidArgument with the reference's message.
 // Prints "host api ok" and exits 0 when everything holds.
@@ -128,6 +130,38 @@ static int join_test(HashingScheme scheme) {
   return 0;
 }
 
+// No-partitioning join (sql-ops/tests/test_no_partitioning_join.rs shape):
+// unique build keys 0..N-1, every probe key among them, probe payload 1, so
+// SUM = the number of probes; grouped by table region (the default; a 16 MB
+// table is two 8 MB regions) and in input order.
+static int hash_join_test(HashingScheme scheme) {
+  const uint64_t nb = 1u << 19, np = 1u << 21;
+  const uint64_t size = 1u << 20;  // 16 MB of int64 entries: two regions
+  const uint32_t grid = 148, block = 256;
+  std::vector<int64_t> rk(nb), sk(np), ones(np, 1);
+  std::iota(rk.begin(), rk.end(), 0);
+  std::shuffle(rk.begin(), rk.end(), std::mt19937_64(3));
+  for (uint64_t i = 0; i < np; ++i) sk[i] = (int64_t)((i * 2654435761u) % nb);
+  auto drk = upload(rk), dsk = upload(sk), dones = upload(ones);
+  for (bool grouped : {true, false}) {
+    HashTable<int64_t> table(size, nullptr);
+    CudaHashJoin<int64_t> hj(scheme, false, table, grid, block, grid, block);
+    hj.set_build_grouping(grouped);
+    hj.set_probe_grouping(grouped);
+    DeviceBuffer<uint64_t> result(grid * block);
+    check_cuda(cudaMemset(result.data(), 0, grid * block * sizeof(uint64_t)), "memset");
+    hj.build(drk.data(), drk.data(), nb, nullptr);
+    hj.probe_sum(dsk.data(), dones.data(), np, result.data(), grid * block, nullptr);
+    check_cuda(cudaDeviceSynchronize(), "sync");
+    hj.status();
+    const auto r = download(result.data(), grid * block);
+    uint64_t sum = 0;
+    for (uint64_t v : r) sum += v;
+    REQUIRE(sum == np);
+  }
+  return 0;
+}
+
 static int error_test() {
   GpuRadixPartitioner p(GpuHistogramAlgorithm::Chunked, GpuRadixPartitionAlgorithm::NC,
                         RadixBits(8), 4, 1024);
@@ -149,6 +183,8 @@ int main() {
     if (partition_test()) return 1;
     if (join_test(HashingScheme::BucketChaining)) return 1;
     if (join_test(HashingScheme::Perfect)) return 1;
+    if (hash_join_test(HashingScheme::LinearProbing)) return 1;
+    if (hash_join_test(HashingScheme::Perfect)) return 1;
     if (error_test()) return 1;
   } catch (const Error &e) {
     std::fprintf(stderr, "error %d: %s\n", e.code(), e.what());
