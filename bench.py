@@ -119,7 +119,7 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-repeats", type=int, default=1,
                     help="serve workload: runs of each arm on the same stream")
-    ap.add_argument("--serve-workers", type=int, default=1,
+    ap.add_argument("--serve-workers", type=int, default=2,
                     help="engines of the server that run large joins at once")
     ap.add_argument("--sweep", default="6,8,10,12,14,16,18",
                     help="radix bits of the partition sweep")

@@ -29,9 +29,10 @@
 //    probe_slice tuples.  A free worker takes the shortest admitted large
 //    join (or one that has waited over 0.5 s); a worker keeps two joins
 //    enqueued on its stream, so the next starts without a host round trip,
-//    and the one after is loaded on a load stream while they run.  Workers overlap with each other and with batches (one worker by
-//    default: two large joins at once each run at half speed, which only
-//    lengthens their latency).
+//    and the one after is loaded on a load stream while they run.  Workers
+//    overlap with each other and with batches.  By default two workers (one
+//    when two engines would take over half the budget): their large joins
+//    fill each other's idle phases (launch gaps, short kernels, tails).
 //  * completion: the scheduler thread polls the done events, releases the
 //    reservation and the relations, and hands responses to waiters.
 #include <algorithm>
@@ -642,7 +643,11 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
   if (cfg) s->cfg = *cfg;
   fi_join_server_config &c = s->cfg;
   if (!c.hbm_budget_bytes) c.hbm_budget_bytes = 150000000000ull;
-  if (!c.workers) c.workers = 1;
+  // 0: two workers when their engines take at most half the budget, else
+  // one (measured on the 10,000-request stream: two workers serve 7% more at
+  // 1.2x the plain path's capacity and cut p99 at 0.8x, 727 -> 500 ms)
+  const bool auto_workers = c.workers == 0;
+  if (auto_workers) c.workers = 2;
   if (!c.small_tuples) c.small_tuples = 4ull << 20;
   if (!c.max_batch_jobs) c.max_batch_jobs = 256;
   if (!c.batch_tuples) c.batch_tuples = 1ull << 25;
@@ -664,13 +669,22 @@ extern "C" int fi_join_server_new(const fi_join_server_config *cfg,
     ce = cudaStreamCreateWithFlags(&s->load_large, cudaStreamNonBlocking);
   if (ce != cudaSuccess) rc = cuda_error(ce, "stream create");
   s->workers.resize(rc ? 0 : c.workers);
-  for (Worker &w : s->workers) {
+  uint64_t first_engine_bytes = 0;
+  for (size_t wi = 0; wi < s->workers.size(); ++wi) {
     if (rc) break;
+    if (auto_workers && wi == 1 && 2 * first_engine_bytes > c.hbm_budget_bytes / 2) {
+      c.workers = 1;  // worker 1 was never set up
+      s->workers.resize(1);
+      break;
+    }
+    Worker &w = s->workers[wi];
     fi_radix_bits caps{{12, 10, -1}};
     rc = fi_radix_join_engine_new(c.max_build, c.probe_slice, 16, caps,
                                   FI_HASHING_BUCKET_CHAINING, &w.engine);
     if (rc) break;
-    s->fixed += fi_radix_join_engine_workspace_bytes(w.engine);
+    const uint64_t engine_bytes = fi_radix_join_engine_workspace_bytes(w.engine);
+    if (wi == 0) first_engine_bytes = engine_bytes;
+    s->fixed += engine_bytes;
     if ((ce = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking)) != cudaSuccess)
       rc = cuda_error(ce, "worker set-up");
     for (Slot &sl : w.slot) {
@@ -802,5 +816,6 @@ extern "C" int fi_join_server_stats_get(fi_join_server *s, fi_join_server_stats 
   *out = s->stats;
   out->reserved_bytes = s->reserved;
   out->peak_reserved_bytes = s->peak;
+  out->workers = s->workers.size();
   return FI_OK;
 }

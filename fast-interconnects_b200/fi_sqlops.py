@@ -951,7 +951,8 @@ class _ServerStatsC(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "submitted", "completed", "batches", "batched_jobs", "engine_runs",
         "reserved_bytes", "peak_reserved_bytes", "fixed_bytes", "arena_bytes")] + [
-        (n, C.c_double) for n in ("engine_busy_us", "batch_busy_us", "enqueue_us")]
+        (n, C.c_double) for n in ("engine_busy_us", "batch_busy_us", "enqueue_us")] + [
+        ("workers", C.c_uint64)]
 
 
 class JoinSource(enum.IntEnum):

@@ -874,7 +874,8 @@ typedef struct {
                                 the workers' engines, the batch arenas and a
                                 slab for the relations it holds (the rest,
                                 capped by the device's free memory) */
-  uint32_t workers;          /* concurrent large joins (0: 1) */
+  uint32_t workers;          /* concurrent large joins (0: 2, or 1 when two
+                                engines would take over half the budget) */
   uint64_t small_tuples;     /* joins below this (|R|+|S|) are batched (0: 4M) */
   uint32_t max_batch_jobs;   /* jobs per batch (0: 256) */
   uint64_t batch_tuples;     /* partition arena of one batch (0: 2^25) */
@@ -921,6 +922,8 @@ typedef struct {
   double engine_busy_us;  /* device time of the large joins (events) */
   double batch_busy_us;   /* device time of the batches (events) */
   double enqueue_us;      /* host time the scheduler spent issuing work */
+  uint64_t workers;       /* engines running large joins (the config's, or
+                             the automatic choice for workers = 0) */
 } fi_join_server_stats;
 
 /* Starts a server on the current device: allocates the workers' engines and

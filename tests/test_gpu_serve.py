@@ -52,6 +52,37 @@ def test_server_mixed_stream_equals_alone(fi):
         assert (g["sum"] & MASK, g["count"]) == synthetic_expected(fi, tb, rn, sn, seed, z)
 
 
+def test_server_automatic_workers(fi):
+    """workers = 0 picks two engines when they take at most half the budget
+    and one otherwise; either way the results equal the closed form."""
+    shape = dict(max_build=1 << 24, probe_slice=1 << 24, batch_tuples=1 << 20)
+    one = fi.JoinServer(hbm_budget_bytes=60 << 30, workers=1, **shape)
+    fixed1 = one.stats()["fixed_bytes"]
+    one.close()
+    two = fi.JoinServer(hbm_budget_bytes=60 << 30, workers=0, **shape)
+    st = two.stats()
+    assert st["workers"] == 2
+    engine = st["fixed_bytes"] - fixed1  # one engine's workspace
+    reqs = [(16, 3 << 20, 6 << 20, 77, 0.0), (8, 5 << 20, 5 << 20, 78, 1.0)]
+    got = [two.wait(two.submit(tuple_bytes=tb, source=fi.JoinSource.Synthetic,
+                               build_len=rn, probe_len=sn, seed=seed, zipf_s=z))
+           for tb, rn, sn, seed, z in reqs]
+    two.close()
+    for (tb, rn, sn, seed, z), g in zip(reqs, got):
+        assert g["status"] == 0
+        assert (g["sum"] & MASK, g["count"]) == synthetic_expected(fi, tb, rn, sn, seed, z)
+    # a budget that holds one engine, the batch arenas and a 1 GB slab
+    budget = fixed1 + (1 << 30)
+    tight = fi.JoinServer(hbm_budget_bytes=budget, workers=0, **shape)
+    assert tight.stats()["workers"] == (1 if 2 * engine > budget // 2 else 2)
+    g = tight.wait(tight.submit(tuple_bytes=16, source=fi.JoinSource.Synthetic,
+                                build_len=1 << 20, probe_len=1 << 21, seed=79))
+    tight.close()
+    assert g["status"] == 0
+    assert (g["sum"] & MASK, g["count"]) == synthetic_expected(fi, 16, 1 << 20, 1 << 21,
+                                                              79, 0.0)
+
+
 def test_server_device_source_alone_vs_mix(fi, oracle):
     """Device-resident relations (with misses): the response of a request
     submitted alone equals its response inside a mix, and the engine's."""
