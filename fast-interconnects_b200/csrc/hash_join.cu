@@ -472,6 +472,8 @@ struct Window32<int32_t> {
 };
 
 // kWindowed: the table base is 32-byte aligned (else slot by slot, W = 1).
+constexpr uint32_t kProbeThreads = 256;
+
 template <typename K, bool kWindowed>
 __global__ void ht_probe_grouped_kernel(const Tuple<K> *__restrict__ ht,
                                         uint64_t size, int scheme,
@@ -479,7 +481,8 @@ __global__ void ht_probe_grouped_kernel(const Tuple<K> *__restrict__ ht,
                                         const K *__restrict__ key,
                                         const K *__restrict__ pay,
                                         const uint32_t *skip, uint64_t len,
-                                        uint64_t *__restrict__ result) {
+                                        uint64_t *__restrict__ result,
+                                        uint64_t result_len) {
   // a skewed slice was left in input order: probe the columns instead
   const bool in_order = *skip != 0;
   using Win = Window32<K>;
@@ -540,7 +543,11 @@ __global__ void ht_probe_grouped_kernel(const Tuple<K> *__restrict__ ht,
       if (slot < size && ht[slot].key == p.key) sum += v;
     }
   }
-  result[gid] += sum;
+  // the library's own grid: thread sums land modulo the caller's
+  // grid * block entries of result_set, whose total is the join's sum
+  if (sum)
+    atomicAdd(reinterpret_cast<unsigned long long *>(result + gid % result_len),
+              static_cast<unsigned long long>(sum));
 }
 
 // Region bits of a table: regions of at most kRegionBytes; 0 when the whole
@@ -666,6 +673,17 @@ cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size
                                     uint32_t sm_count, cudaStream_t stream) {
   Tuple<K> *out = static_cast<Tuple<K> *>(tuples);
   uint32_t *skip = region_scratch + 2;  // after the status and the build's counter
+  // The library's launch shape, whatever the caller's probe grid: probes
+  // served from L2 need every SM full of warps to hide its latency (the
+  // caller's grid * block still sizes result_set).
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, (const void *)ht_probe_grouped_kernel<K, true>,
+          (int)kProbeThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const uint32_t probe_grid = (uint32_t)per_sm * sm_count;
+  const uint64_t result_len = (uint64_t)grid * block;
   for (uint64_t s0 = 0; s0 < len; s0 += slice) {
     const uint64_t n = min(slice, len - s0);
     cudaError_t e = group_by_region<K>(scheme, ht_size, key + s0, pay + s0, n,
@@ -673,13 +691,13 @@ cudaError_t launch_ht_probe_grouped(int scheme, const void *ht, uint64_t ht_size
                                        skip, stream);
     if (e != cudaSuccess) return e;
     if (reinterpret_cast<uintptr_t>(ht) % 32 == 0)
-      ht_probe_grouped_kernel<K, true><<<grid, block, 0, stream>>>(
+      ht_probe_grouped_kernel<K, true><<<probe_grid, kProbeThreads, 0, stream>>>(
           static_cast<const Tuple<K> *>(ht), ht_size, scheme, out, key + s0,
-          pay + s0, skip, n, result);
+          pay + s0, skip, n, result, result_len);
     else
-      ht_probe_grouped_kernel<K, false><<<grid, block, 0, stream>>>(
+      ht_probe_grouped_kernel<K, false><<<probe_grid, kProbeThreads, 0, stream>>>(
           static_cast<const Tuple<K> *>(ht), ht_size, scheme, out, key + s0,
-          pay + s0, skip, n, result);
+          pay + s0, skip, n, result, result_len);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

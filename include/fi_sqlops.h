@@ -430,8 +430,12 @@ int fi_cuda_hash_join_probe_sum_int64(fi_cuda_hash_join *hj,
  * no host round trip.  On by default with slices of 2^27 tuples; each slice
  * takes slice * tuple_bytes bytes of scratch that the handle keeps, so
  * builds and probes of one handle whose work overlaps on the GPU (different
- * streams) race on it: order them, as the table itself requires.
- * enable = 0 probes in input order with no scratch. */
+ * streams) race on it: order them, as the table itself requires.  The
+ * grouped probe runs with the library's own launch shape (every SM full of
+ * warps) and adds each of its threads' sums into result_set[thread modulo
+ * probe_grid * probe_block], so the entries' total is the join's sum, as
+ * with the caller's grid.  enable = 0 probes in input order with no scratch,
+ * on the probe grid. */
 int fi_cuda_hash_join_set_probe_grouping(fi_cuda_hash_join *hj, int enable,
                                          uint64_t slice_tuples);
 

@@ -283,6 +283,34 @@ def test_hash_join_grouped_probe_skewed(fi, oracle, ndt, tdt, scheme, slice_):
 
 
 @pytest.mark.parametrize("ndt,tdt", DTYPES)
+@pytest.mark.parametrize("scheme", ["LinearProbing", "Perfect"])
+def test_hash_join_grouped_probe_small_result_set(fi, oracle, ndt, tdt, scheme):
+    """The grouped probe runs on the library's own grid and folds its
+    threads' sums into the caller's grid * block entries (here 3 x 96, far
+    fewer than its threads): their total is the oracle's sum."""
+    rng = np.random.default_rng(61)
+    size = 1 << 21 if ndt == np.int64 else 1 << 22  # 32 MB tables
+    n_b = size // 2
+    r_key = rng.permutation(size)[:n_b].astype(ndt)
+    r_pay = rng.integers(-1000, 1000, n_b).astype(ndt)
+    n_p = 2 * size + 5
+    s_key = rng.integers(0, size + 10, n_p).astype(ndt)
+    s_pay = rng.integers(-(1 << 20), 1 << 20, n_p).astype(ndt)
+    ht = fi.HashTable(size, tdt)
+    hj = fi.CudaHashJoin(getattr(fi.HashingScheme, scheme), ht, (3, 96), (3, 96))
+    hj.build(to_dev(r_key), to_dev(r_pay))
+    res = torch.zeros(3 * 96, dtype=torch.int64, device="cuda")
+    hj.probe_sum(to_dev(s_key), to_dev(s_pay), res)
+    hj.status()
+    got = int(to_host(res).astype(np.uint64).sum(dtype=np.uint64))
+    if scheme == "LinearProbing":
+        exp, _ = oracle.ht_linearprobing_sum(r_key, r_pay, s_key, s_pay, size)
+    else:
+        exp, _ = oracle.ht_perfect_sum(r_key, r_pay, s_key, s_pay, size)
+    assert got == exp
+
+
+@pytest.mark.parametrize("ndt,tdt", DTYPES)
 @pytest.mark.parametrize("offset", [0, 1])
 def test_hash_join_grouped_probe_table_alignment(fi, oracle, ndt, tdt, offset):
     """The grouped linear-probing probe reads 32-byte windows of the table
