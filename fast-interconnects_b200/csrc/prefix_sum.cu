@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "tma_scatter.cuh"
 
 namespace fi {
 
@@ -228,6 +229,107 @@ __global__ void __launch_bounds__(kClusterThreads)
   cluster.sync();
   uint32_t *gh = g_hist + (uint64_t)c * F + (uint64_t)q * kBins;
   for (uint32_t p = threadIdx.x; p < kBins; p += blockDim.x)
+    if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
+}
+
+// Histogram of fanouts above 2^15 fed by TMA: one 1024-thread CTA per
+// (chunk, split, bin range) holds the range's 2^15 counters (128 KB) and
+// streams its split's keys through two 32 KB shared-memory stages with 1-D
+// bulk copies (cp.async.bulk + mbarrier), so every SM keeps a tile in flight
+// while it counts the previous one.  The range CTAs of one split are
+// adjacent in the grid, so the rereads of each tile mostly come from L2.
+// The bin-range kernel above reads the same keys with 512 threads and a few
+// 16-byte loads in flight each and is latency-bound (2.0 ms for 2^16 bins,
+// 7.8 ms for 2^18, over 512M keys).  Waits are bounded; a wait that gives up records
+// kDevErrTimeout in *status (when given), drains the copies in flight and
+// leaves the CTA's counts out.  Every range rereads the split's keys, so
+// the cost grows with the ranges: 1.82 ms for two (2^16 bins), 3.61 ms for
+// four (2^17) and 7.1-7.2 ms for eight (2^18) over 512M int64 keys, the
+// same for uniform and Zipf-skewed keys.
+template <typename K>
+struct RangeTile {
+  static constexpr uint32_t kThreads = 1024;
+  static constexpr uint32_t kKeys = (32u << 10) / sizeof(K);  // one 32 KB stage
+  static constexpr uint32_t kStages = 2;
+};
+
+template <typename K>
+size_t range_tma_smem() {
+  return 64 + RangeTile<K>::kStages * (size_t)(32u << 10) +
+         ((size_t)sizeof(uint32_t) << kHistSmemBinsLog2);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(1024, 1)
+    histogram_range_tma_kernel(const K *__restrict__ keys, uint64_t len,
+                               uint64_t clen, uint32_t chunks, uint32_t splits,
+                               uint32_t ranges, uint32_t radix_bits,
+                               uint32_t ignore_bits, uint32_t *__restrict__ g_hist,
+                               int *status) {
+  using T = RangeTile<K>;
+  constexpr uint32_t kBins = 1u << kHistSmemBinsLog2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  K *stages = reinterpret_cast<K *>(smem_raw + 64);
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(smem_raw + 64 + T::kStages * (32u << 10));
+  const uint32_t F = 1u << radix_bits;
+  const uint64_t mask = static_cast<uint64_t>(F - 1u) << ignore_bits;
+  const uint32_t r = blockIdx.x % ranges;
+  const uint32_t sp = (blockIdx.x / ranges) % splits;
+  const uint32_t c = blockIdx.x / (ranges * splits);
+  const uint32_t bin_lo = r * kBins;
+  uint64_t sb, se;
+  split_range<K>(len, clen, chunks, c, splits, sp, sb, se);
+  const uint32_t tid = threadIdx.x;
+  for (uint32_t i = tid; i < kBins; i += blockDim.x) cnt[i] = 0;
+  if (tid == 0) {
+    for (uint32_t st = 0; st < T::kStages; ++st) mbar_init(&bars[st], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // [sb, se) starts 16-byte aligned; each tile's 16-byte multiple comes by
+  // TMA, the last tile's ragged end (under 16 bytes) by plain loads
+  const uint64_t n_all = se > sb ? se - sb : 0;
+  const uint64_t ntiles = (n_all + T::kKeys - 1) / T::kKeys;
+  auto issue = [&](uint64_t t) {
+    const uint64_t t0 = sb + t * T::kKeys;
+    const uint32_t n = (uint32_t)min((uint64_t)T::kKeys, se - t0);
+    const uint32_t bytes = (n * (uint32_t)sizeof(K)) & ~15u;
+    uint64_t *bar = &bars[t % T::kStages];
+    mbar_arrive_expect_tx(bar, bytes);
+    if (bytes) bulk_g2s(stages + (t % T::kStages) * T::kKeys, keys + t0, bytes, bar);
+  };
+  if (tid == 0 && ntiles > 0) issue(0);
+  bool counted = true;
+  for (uint64_t t = 0; t < ntiles; ++t) {
+    if (tid == 0 && t + 1 < ntiles) {
+      fence_proxy_async_smem();  // every thread left that stage before the last barrier
+      issue(t + 1);
+    }
+    const bool ok = mbar_wait(&bars[t % T::kStages], (uint32_t)((t / T::kStages) & 1u));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        record_error(status, kDevErrTimeout);
+        tma_drain<T::kStages>(bars, t, ntiles);
+      }
+      __syncthreads();
+      counted = false;
+      break;
+    }
+    const uint64_t t0 = sb + t * T::kKeys;
+    const uint32_t n = (uint32_t)min((uint64_t)T::kKeys, se - t0);
+    const uint32_t n_tma = ((n * (uint32_t)sizeof(K)) & ~15u) / (uint32_t)sizeof(K);
+    const K *stage = stages + (t % T::kStages) * T::kKeys;
+    for (uint32_t i = tid; i < n; i += T::kThreads) {
+      const K k = i < n_tma ? stage[i] : load_cs(keys + t0 + i);
+      const uint32_t b = key_to_partition(k, mask, ignore_bits) - bin_lo;
+      if (b < kBins) atomicAdd(&cnt[b], 1u);
+    }
+    __syncthreads();  // the stage is free for the copy of tile t + 2
+  }
+  if (!counted) return;
+  uint32_t *gh = g_hist + (uint64_t)c * F + bin_lo;
+  for (uint32_t p = tid; p < kBins; p += blockDim.x)
     if (cnt[p] != 0) atomicAdd(&gh[p], cnt[p]);
 }
 
@@ -462,17 +564,36 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
                               (int)bytes);
 }
 
-// Histogram of a fanout above 2^15 into g_hist (zeroed by the caller):
-// the cluster kernel when the GPU can schedule its clusters, else the
-// bin-range kernel.
+// Histogram of a fanout above 2^15 into g_hist (zeroed by the caller): the
+// TMA-fed bin-range kernel for a 16-byte aligned key column without a
+// column copy; else, at 2^18 bins, the cluster kernel when the GPU can
+// schedule its clusters; else the bin-range kernel.
 template <typename K>
 static cudaError_t launch_wide_histogram(const K *keys, const K *pays,
                                          K *dst_key, K *dst_pay, uint64_t len,
                                          uint64_t clen, uint32_t chunks,
                                          uint32_t splits, uint32_t radix_bits,
                                          uint32_t ignore_bits, uint32_t pad,
-                                         uint32_t *g_hist, cudaStream_t stream) {
+                                         uint32_t *g_hist, int *status,
+                                         cudaStream_t stream) {
   const uint32_t ranges = hist_ranges(radix_bits);
+  const size_t tsm = range_tma_smem<K>();
+  // measured on B200, 512M int64 keys over 148 chunks: 1.82 ms at 2^16
+  // bins, 3.61 ms at 2^17, 7.19 ms at 2^18 for uniform keys and 7.11 ms
+  // for Zipf(1.5) keys (every range pass rereads the keys at ~4.8 TB/s);
+  // the cluster kernel below takes 7.03 ms at 2^18 for uniform keys but
+  // 9.5 ms for Zipf(1.0) and 19.0 ms for Zipf(1.5), whose hot bin
+  // serialises the remote atomics
+  if (dst_key == nullptr && reinterpret_cast<uintptr_t>(keys) % 16 == 0 &&
+      tsm <= (size_t)device_max_smem_optin()) {
+    cudaError_t e = set_smem<K>((const void *)histogram_range_tma_kernel<K>, tsm);
+    if (e != cudaSuccess) return e;
+    histogram_range_tma_kernel<K><<<chunks * splits * ranges, RangeTile<K>::kThreads,
+                                    tsm, stream>>>(keys, len, clen, chunks, splits,
+                                                   ranges, radix_bits, ignore_bits,
+                                                   g_hist, status);
+    return cudaGetLastError();
+  }
   // measured on B200, 512M keys over 148 chunks: at 2^16 bins the two-range
   // kernel takes 2.0 ms and the cluster 3.0 ms (its remote shared-memory
   // atomics cost more than the second, mostly L2-served, key read); at 2^18
@@ -545,7 +666,7 @@ cudaError_t launch_chunked_prefix_sum(const K *keys, uint64_t len,
   if (ranges > 1) {
     e = launch_wide_histogram<K>(keys, nullptr, nullptr, nullptr, len, clen,
                                  chunks, splits, radix_bits, ignore_bits, pad,
-                                 s.hist, stream);
+                                 s.hist, s.status, stream);
   } else {
     histogram_kernel<K><<<chunks * splits, kHistThreads, sm, stream>>>(
         keys, nullptr, nullptr, nullptr, len, clen, chunks, splits, 1,
@@ -602,7 +723,7 @@ cudaError_t launch_contiguous_prefix_sum(const K *keys, const K *pays,
   if (ranges > 1) {
     e = launch_wide_histogram<K>(keys, pays, dst_key, dst_pay, len, clen, grid,
                                  splits, radix_bits, ignore_bits, pad, s.hist,
-                                 stream);
+                                 s.status, stream);
     if (e != cudaSuccess) return e;
   } else {
     histogram_kernel<K><<<grid * splits, kHistThreads, sm, stream>>>(
