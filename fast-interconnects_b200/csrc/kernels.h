@@ -18,7 +18,7 @@ struct HistScratch {
   int *status;           // [1] device error word (0 = ok)
 };
 
-constexpr uint32_t kScanTile = 1024;  // partitions per look-back tile
+constexpr uint32_t kScanTile = 32;  // partitions per look-back tile
 
 // Number of CTAs that share one chunk in the histogram kernels.
 uint32_t hist_splits(uint32_t chunks, uint32_t sm_count);
