@@ -103,6 +103,38 @@ def test_errors_without_launch(fi):
     assert "pass is not specified" in str(e.value)
 
 
+def test_hash_join_grouping_arguments(fi):
+    """The grouping switches of CudaHashJoin validate their slices on the
+    host; the status of a handle that never grouped is FI_OK (no device
+    work).  The handle is made on a placeholder table address: nothing here
+    touches the device."""
+    L = fi.lib()
+    h = C.c_void_p()
+    table = C.c_void_p(0x100000)
+    fi._check(L.fi_cuda_hash_join_new(C.c_int(int(fi.HashingScheme.LinearProbing)),
+                                      C.c_int(0), table, C.c_uint64(1 << 20),
+                                      C.c_uint64(1 << 20), C.c_uint32(148),
+                                      C.c_uint32(256), C.c_uint32(148),
+                                      C.c_uint32(256), C.byref(h)))
+    try:
+        for setter in (L.fi_cuda_hash_join_set_build_grouping,
+                       L.fi_cuda_hash_join_set_probe_grouping):
+            with pytest.raises(fi.SqlOpsError) as e:
+                fi._check(setter(h, C.c_int(1), C.c_uint64(0)))
+            assert e.value.kind == "InvalidArgument" and "at least 1" in str(e.value)
+            with pytest.raises(fi.SqlOpsError) as e:
+                fi._check(setter(h, C.c_int(1), C.c_uint64(1 << 32)))
+            assert e.value.kind == "InvalidArgument" and "below 2^32" in str(e.value)
+            fi._check(setter(h, C.c_int(1), C.c_uint64(1_000_003)))
+            fi._check(setter(h, C.c_int(0), C.c_uint64(0)))  # off: the slice is unused
+        fi._check(L.fi_cuda_hash_join_status(h))
+        with pytest.raises(fi.SqlOpsError) as e:
+            fi._check(L.fi_cuda_hash_join_status(None))
+        assert e.value.kind == "InvalidArgument"
+    finally:
+        L.fi_cuda_hash_join_free(h)
+
+
 def test_autotune_model_and_table(fi, tmp_path):
     """The autotuner's model (no table) and a loaded table (no GPU needed)."""
     fi.autotune_load(None)
