@@ -18,8 +18,9 @@
 // 2^25-entry, 512 MB table: one random access per probe, far beyond the
 // 126 MB L2), perfect hashing probes in 4.7 ms (16M + 1 entries); grouped by
 // table region (below, the default), the linear-probing build takes 0.57 ms
-// and the probe 4.2 ms, the perfect probe 3.2 ms.  In input order, four tuples per thread with
-// their table loads issued together made it no faster (11.7 ms), nor did
+// and the probe 4.2-4.5 ms, the perfect probe 3.2 ms.  In input order, four
+// tuples per thread with their table loads issued together made it no
+// faster (11.7 ms), nor did
 // loading a window of 4 slots (64 B) per step instead of slot by slot (11.0
 // ms): the probe is bound by the rate of random HBM accesses (about 30 G/s
 // reach DRAM in both schemes), and the perfect table is faster because it is
